@@ -1,0 +1,241 @@
+/*
+ * xac.h — C ABI of libxac.so, the B200 (sm_100a) coupled fluid + thermal
+ * lattice-Boltzmann solver that drops in for tgautam03/xAdvCool's solver path.
+ *
+ * Plain C: pointers, sizes, ints and doubles only. Streams are passed as
+ * `void*` holding a cudaStream_t (NULL = the legacy default stream). Every
+ * function returns an int status (XAC_OK on success); on failure
+ * xac_last_error() returns a message for the calling thread. No C++ exception
+ * crosses this boundary.
+ *
+ * Layouts seen by callers are the reference's:
+ *   scalar fields  [nx][ny][nz]        float32, z fastest (wp.array3d)
+ *   velocity       [nx][ny][nz][3]     float32 (wp.array3d of vec3f)
+ *   populations    [19][nx][ny][nz]    float32 (wp.array4d)
+ *   mask           [nx][ny][nz]        int32, values XAC_BC_*
+ * The D3Q19 direction order, weights and opposite map are the reference's
+ * (src/fluid_engine3d.py:11-53).
+ */
+#ifndef XAC_H
+#define XAC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define XAC_OK 0
+#define XAC_EINVAL 1     /* bad argument (null pointer, bad size, bad enum)        */
+#define XAC_ECUDA 2      /* a CUDA runtime call failed                             */
+#define XAC_EDIVERGED 3  /* the divergence guard fired (NaN, |u|>0.17, T>1e4)      */
+#define XAC_ETIMEOUT 4   /* a bounded device-side wait gave up                     */
+#define XAC_ENOMEM 5     /* device allocation failed                               */
+
+/* ---- cell labels: src/fluid_engine3d.py:11-14 / src/geometry.py:9-12 ------ */
+#define XAC_BC_FLUID 0
+#define XAC_BC_SOLID 1
+#define XAC_BC_INLET 2
+#define XAC_BC_OUTLET 3
+
+/* ---- population storage precision of a lattice ---------------------------- */
+#define XAC_FP32 0  /* the reference's float32 populations                          */
+#define XAC_FP16 1  /* binary16 deviations from the rest equilibrium, float32 maths  */
+#define XAC_BF16 2  /* bfloat16 deviations from the rest equilibrium, float32 maths  */
+
+/* ---- stats vector (xac_stats): src/fluid_engine3d.py:283 index order, then
+ *      src/thermal_engine3d.py:228 order, then one extra slot ---------------- */
+#define XAC_ST_MAX_V 0
+#define XAC_ST_SUM_V 1
+#define XAC_ST_SUM_KE 2       /* sum of |u|^2 over ALL cells (no 1/2), fluid_engine3d.py:292 */
+#define XAC_ST_COUNT 3
+#define XAC_ST_SUM_RHO 4
+#define XAC_ST_SUM_RHO_IN 5   /* plane x = 1 */
+#define XAC_ST_SUM_RHO_OUT 6  /* plane x = nx-2 */
+#define XAC_ST_SUM_UX_OUT 7   /* outlet cells */
+#define XAC_ST_C_IN 8
+#define XAC_ST_C_OUT 9
+#define XAC_ST_C_OUTLET 10
+#define XAC_ST_MAX_T 11
+#define XAC_ST_SUM_T 12
+#define XAC_ST_COUNT_T 13
+#define XAC_ST_Q_OUT 14       /* sum of u_x*T over outlet cells */
+#define XAC_ST_Q_OUT_COUNT 15
+#define XAC_ST_NONFINITE 16   /* cells whose |u| or T is not finite */
+#define XAC_NSTATS 17
+
+/* ---- scalar outputs (xac_scalars): generate_dataset.py:57-179 plus the
+ *      Parquet-only quantities of generate_dataset.py:538-579 ------------------ */
+#define XAC_SC_DP 0                /* delta_P over non-solid cells, :99-108        */
+#define XAC_SC_RTH 1               /* R_th, :113-140                               */
+#define XAC_SC_NU 2                /* Nu, :145-155                                 */
+#define XAC_SC_F_FRICTION 3
+#define XAC_SC_P_PUMP 4
+#define XAC_SC_COP 5
+#define XAC_SC_Q_VOL 6
+#define XAC_SC_T_MAX_SURFACE 7
+#define XAC_SC_T_AVG_SURFACE 8
+#define XAC_SC_DELTA_T_MAX 9
+#define XAC_SC_SIGMA_T 10
+#define XAC_SC_FLUID_TEMP_RISE 11
+#define XAC_SC_PRESSURE_DROP_ALL 12  /* Parquet column pressure_drop: all cells of the planes, :556 */
+#define XAC_SC_MAX_VELOCITY 13
+#define XAC_SC_MAX_TEMPERATURE 14
+#define XAC_SC_MEAN_TEMPERATURE 15
+#define XAC_SC_DH 16               /* compute_hydraulic_diameter, :57-68           */
+#define XAC_SC_V_FLUID 17
+#define XAC_SC_A_WETTED 18
+#define XAC_SC_POROSITY 19         /* compute_porosity, :71-74                     */
+#define XAC_SC_Q_ABSORBED 20       /* intermediate of R_th / Nu, :133-136          */
+#define XAC_SC_DT_CONV 21          /* T_avg_surface - T_fluid_avg, :148            */
+#define XAC_SC_RHO_AVG 22          /* intermediate of f_friction, :160             */
+#define XAC_NSCALARS 23
+
+const char *xac_last_error(void);
+int xac_version(void);
+
+/* ========================================================================== *
+ * Unfused per-operator entry points, reference layout, caller-owned DEVICE
+ * pointers, launched on `stream`. Each replaces one Warp kernel launch
+ * (wp.launch(kernel, dim=(nx,ny,nz), inputs=[...])) with the same inputs.
+ * ========================================================================== */
+
+/* src/fluid_engine3d.py:58-80 compute_equilibrium_kernel(rho, u, f_eq) */
+int xac_equilibrium(const float *rho, const float *u, float *f_eq, int nx, int ny, int nz, void *stream);
+/* src/fluid_engine3d.py:85-113 compute_macroscopic_kernel(f, rho, u) */
+int xac_macroscopic(const float *f, float *rho, float *u, int nx, int ny, int nz, void *stream);
+/* src/fluid_engine3d.py:118-136 bgk_collision_kernel(f_old, f_eq, f_post, mask, tau) */
+int xac_bgk_collision(const float *f_old, const float *f_eq, float *f_post, const int32_t *mask, float tau,
+                      int nx, int ny, int nz, void *stream);
+/* src/fluid_engine3d.py:141-176 fused_equilibrium_collision_kernel(f_old, rho, u, f_post, mask, tau) */
+int xac_fused_collision(const float *f_old, const float *rho, const float *u, float *f_post, const int32_t *mask,
+                        float tau, int nx, int ny, int nz, void *stream);
+/* src/fluid_engine3d.py:181-272 streaming_kernel(f_post, f_streamed, mask, u_inlet[1], rho_outlet, nx, ny, nz);
+ * u_inlet is a device pointer to one float, read inside the kernel as the reference does. */
+int xac_stream(const float *f_post, float *f_streamed, const int32_t *mask, const float *u_inlet, float rho_outlet,
+               int nx, int ny, int nz, void *stream);
+/* src/fluid_engine3d.py:277-312 compute_stats_kernel + src/thermal_engine3d.py:226-243 compute_thermal_stats_kernel,
+ * merged and made deterministic (FP64 block reductions, fixed combine order). out_host receives XAC_NSTATS doubles;
+ * the call synchronises `stream`. */
+int xac_stats_fields(const float *rho, const float *u, const float *T, const int32_t *mask, int nx, int ny, int nz,
+                     double *out_host, void *stream);
+
+/* src/thermal_engine3d.py:7-47 compute_thermal_equilibrium_kernel(rho, u, T, g_eq, mask) (rho unused, as there) */
+int xac_thermal_equilibrium(const float *u, const float *T, float *g_eq, const int32_t *mask, int nx, int ny, int nz,
+                            void *stream);
+/* src/thermal_engine3d.py:49-86 thermal_bgk_collision_kernel(g_old, g_eq, g_new, mask, tau_f, tau_s, hs, power) */
+int xac_thermal_bgk_collision(const float *g_old, const float *g_eq, float *g_new, const int32_t *mask,
+                              float tau_fluid, float tau_solid, const float *heat_source, float heat_power, int nx,
+                              int ny, int nz, void *stream);
+/* src/thermal_engine3d.py:91-145 fused_thermal_equilibrium_collision_kernel(g_old, u, T, g_new, mask, ...) */
+int xac_fused_thermal_collision(const float *g_old, const float *u, const float *T, float *g_new,
+                                const int32_t *mask, float tau_fluid, float tau_solid, const float *heat_source,
+                                float heat_power, int nx, int ny, int nz, void *stream);
+/* src/thermal_engine3d.py:147-211 thermal_streaming_kernel(g_post, g_streamed, mask, T_inlet, nx, ny, nz) */
+int xac_thermal_stream(const float *g_post, float *g_streamed, const int32_t *mask, float T_inlet, int nx, int ny,
+                       int nz, void *stream);
+/* src/thermal_engine3d.py:214-224 compute_thermal_macroscopic_kernel(g, T) */
+int xac_thermal_macroscopic(const float *g, float *T, int nx, int ny, int nz, void *stream);
+
+/* Test-only operators of validate_analytical.py (kept off the product path). */
+/* validate_analytical.py:21-30 dirichlet_thermal_bc_kernel(g, T_val, x_plane, ny, nz) */
+int xac_test_dirichlet_plane(float *g, float T_val, int x_plane, int nx, int ny, int nz, void *stream);
+/* validate_analytical.py:255-273 periodic_streaming_kernel and :607-621 periodic_thermal_streaming_kernel */
+int xac_test_periodic_stream(const float *f_post, float *f_streamed, int nx, int ny, int nz, void *stream);
+/* validate_analytical.py:377-395 forced_bgk_collision_kernel(f_old, f_eq, f_new, mask, tau, force_x) */
+int xac_test_forced_bgk(const float *f_old, const float *f_eq, float *f_new, const int32_t *mask, float tau,
+                        float force_x, int nx, int ny, int nz, void *stream);
+/* validate_analytical.py:397-420 periodic_streaming_with_solids_kernel(f_post, f_streamed, mask, nx, ny, nz) */
+int xac_test_periodic_stream_solids(const float *f_post, float *f_streamed, const int32_t *mask, int nx, int ny,
+                                    int nz, void *stream);
+/* validate_analytical.py:502-538 couette_streaming_kernel(f_post, f_streamed, mask, u_wall_x, nx, ny, nz) */
+int xac_test_couette_stream(const float *f_post, float *f_streamed, const int32_t *mask, float u_wall_x, int nx,
+                            int ny, int nz, void *stream);
+
+/* ========================================================================== *
+ * Lattice object: the fused coupled step behind src/simulation.py:14-162.
+ * The library owns the population buffers; caller pointers are borrowed for
+ * the duration of a call. One lattice per stream; calls on different
+ * lattices are thread-safe.
+ * ========================================================================== */
+typedef struct xac_lattice xac_lattice;
+
+typedef struct xac_desc {
+    int nx, ny, nz;
+    const int32_t *mask;       /* HOST, [nx][ny][nz], XAC_BC_* labels (simulation.py:65)                    */
+    const float *heat_source;  /* HOST, [nx][ny][nz] or NULL = 1 on the z=0 plane; normalised to max 1 here
+                                  (simulation.py:77-86)                                                       */
+    double tau_fluid;          /* fluid relaxation time                                                      */
+    double Pr, k_ratio;        /* thermal taus derived as simulation.py:70-71                                */
+    double u_inlet;            /* inlet velocity u_x (simulation.py:62)                                      */
+    double rho_outlet;         /* outlet density (simulation.py:61, 1.0)                                     */
+    double t_inlet;            /* inlet temperature and cold-start T (simulation.py:73)                      */
+    double heat_power;         /* multiplies the normalised heat source (thermal_engine3d.py:117)            */
+    int precision;             /* XAC_FP32 / XAC_FP16 / XAC_BF16                                             */
+} xac_desc;
+
+/* simulation.py:60-90: allocate, derive taus, normalise the heat map, cold-start equilibrium. */
+int xac_lattice_create(const xac_desc *desc, xac_lattice **out, void *stream);
+int xac_lattice_destroy(xac_lattice *lat);
+/* Restart from fields (reference layout, DEVICE pointers, any may be NULL = cold-start value): populations are
+ * set to the equilibria of (rho, u) and (T, u) exactly as simulation.py:89-90 does for the cold start; solid
+ * cells always get rho=1, u=0. This is the warm-start initialiser. */
+int xac_lattice_init_fields(xac_lattice *lat, const float *rho, const float *u, const float *T, void *stream);
+/* Advance n coupled steps; each equals one replay of the reference's 6-kernel graph (simulation.py:93-100). */
+int xac_lattice_step(xac_lattice *lat, int n, void *stream);
+/* Stats of the current step (same quantities as simulation.py:124-129), FP64, deterministic; synchronises. */
+int xac_lattice_stats(xac_lattice *lat, double out_host[XAC_NSTATS], void *stream);
+/* Current macroscopic fields into caller DEVICE buffers, reference layout; any pointer may be NULL. */
+int xac_lattice_fields(xac_lattice *lat, float *rho, float *u, float *T, void *stream);
+/* Inlet velocity as seen by the streaming step (simulation.py:62, :146 for the pump controller). */
+int xac_lattice_set_inlet(xac_lattice *lat, double u_inlet, void *stream);
+int xac_lattice_get_inlet(xac_lattice *lat, double *u_inlet, void *stream);
+int xac_lattice_steps_done(const xac_lattice *lat, long long *steps);
+/* Inputs of generate_dataset.py:80 compute_macroscopic_metrics that are not fields. */
+typedef struct xac_scalar_params {
+    int buf;            /* inlet/outlet buffer length along x (10, generate_dataset.py:90)            */
+    int core_nx;        /* heated core extent (src/geometry.py:15: 128, 128)                          */
+    int core_ny;
+    double t_inlet;     /* 25.0 (generate_dataset.py:88)                                              */
+    double tau_fluid;   /* params["tau_fluid"], for k_fluid (:151-152)                                */
+    double Pr;          /* (:80)                                                                      */
+    double u_inlet;     /* params["u_inlet_val"], for the friction factor (:159)                      */
+} xac_scalar_params;
+
+/* generate_dataset.py:57-179 on the current fields, FP64 on the device; writes XAC_NSCALARS doubles and
+ * synchronises `stream`. */
+int xac_lattice_scalars(xac_lattice *lat, const xac_scalar_params *params, double out_host[XAC_NSCALARS],
+                        void *stream);
+/* The same on caller fields (reference layout, DEVICE pointers; mask int32). */
+int xac_scalars_fields(const float *rho, const float *u, const float *T, const int32_t *mask, int nx, int ny, int nz,
+                       const xac_scalar_params *params, double out_host[XAC_NSCALARS], void *stream);
+/* Raw population state for checkpoint / restart. */
+int xac_lattice_state_bytes(const xac_lattice *lat, size_t *bytes);
+int xac_lattice_save_state(xac_lattice *lat, void *host_dst, size_t bytes, void *stream);
+int xac_lattice_load_state(xac_lattice *lat, const void *host_src, size_t bytes, void *stream);
+
+/* The whole run_simulation loop (simulation.py:102-162) in native code. */
+typedef struct xac_run_opts {
+    int max_steps;        /* 40000 in the reference signature           */
+    int stats_every;      /* 100                                        */
+    double tol_ke, tol_T; /* relative-rate thresholds                   */
+    int constant_power;   /* 0: constant_flow, 1: constant_power pump   */
+    double target_power;
+} xac_run_opts;
+
+typedef struct xac_run_result {
+    long long steps;
+    int converged, diverged;
+    double d_ke, dT_conv, dQ_conv;
+    double u_inlet_final;
+    double last_stats[XAC_NSTATS];
+} xac_run_result;
+
+int xac_lattice_run(xac_lattice *lat, const xac_run_opts *opts, xac_run_result *res, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XAC_H */

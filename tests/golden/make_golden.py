@@ -1,0 +1,131 @@
+"""Generate tests/golden/*.json from the reference checkout (run in a container that has it; the GPU box
+does not, so the outputs are committed).
+
+* designs.json  — sha256 of generate_mask() for the parameters of selected dataset rows and of a grid of
+                  states, and of the ten heat maps (src/geometry.py, imported with a pyvista stub).
+* metrics.json  — compute_macroscopic_metrics() (generate_dataset.py:80-179, imported with h5py and
+                  src.simulation stubs) on seeded synthetic fields (fields rebuilt by ``synthetic_fields``).
+* parquet_rows.json — stratified rows of dataset/metadata.parquet (inputs and golden scalars of the
+                  reference's GPU runs), excluding gaussian_hotspots rows whose seed is process-salted.
+
+Usage: python tests/golden/make_golden.py [/path/to/reference]
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import sys
+import types
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+
+
+def synthetic_fields(seed: int, shape=(148, 128, 32)):
+    """Smooth seeded fields in the ranges of converged solutions (rho ~ 1, |u| < 0.1, T in 25..40)."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = shape
+    x = np.linspace(0, 1, nx)[:, None, None]
+    y = np.linspace(0, 1, ny)[None, :, None]
+    z = np.linspace(0, 1, nz)[None, None, :]
+    a = rng.uniform(0.5, 2.0, size=8)
+    rho = (1.0 + 0.01 * a[0] * (1 - x) + 0.002 * np.sin(6 * a[1] * y) * np.cos(5 * z)).astype(np.float32)
+    u = np.zeros((nx, ny, nz, 3), dtype=np.float32)
+    u[..., 0] = 0.03 * a[2] * np.sin(np.pi * y) * np.sin(np.pi * z) + 0.001 * np.cos(7 * a[3] * x)
+    u[..., 1] = 0.005 * np.sin(9 * a[4] * x) * np.cos(4 * y)
+    u[..., 2] = 0.004 * np.cos(5 * a[5] * x) * np.sin(3 * z)
+    T = (25.0 + 10.0 * a[6] * (1 - z) * np.exp(-3 * (y - 0.5) ** 2) + 2.0 * a[7] * x).astype(np.float32)
+    T = np.broadcast_to(T, (nx, ny, nz)).copy()
+    rho = np.broadcast_to(rho, (nx, ny, nz)).copy()
+    return rho, u, T
+
+
+def _sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def _import_reference(ref: Path):
+    sys.path.insert(0, str(ref))
+    sys.modules.setdefault("pyvista", types.ModuleType("pyvista"))
+    sys.modules.setdefault("h5py", types.ModuleType("h5py"))
+    sim = types.ModuleType("src.simulation")
+    sim.run_simulation = None
+    sys.modules["src.simulation"] = sim
+    import src.geometry as geometry  # noqa: E402
+    import generate_dataset as gd  # noqa: E402
+    return geometry, gd
+
+
+def main(ref: Path):
+    import pandas as pd
+    geometry, gd = _import_reference(ref)
+    df = pd.read_parquet(ref / "dataset" / "metadata.parquet")
+
+    # ---- parquet rows: stratified over design family x heat map, reproducible heat maps only
+    rows = []
+    rng = np.random.default_rng(1234)
+    keep = df[df["heat_source_type"] != "gaussian_hotspots"]
+    for (design, hs), grp in keep.groupby(["design_name", "heat_source_type"]):
+        pick = grp.iloc[int(rng.integers(0, len(grp)))]
+        rows.append(pick)
+    cols = ["sample_id", "design_name", "design_idx", "heat_source_type", "feature_size", "spacing", "tau_fluid",
+            "u_inlet_val", "heat_power", "Pr", "k_ratio", "porosity", "Dh", "Re", "max_velocity", "max_temperature",
+            "mean_temperature", "pressure_drop", "sim_steps", "converged", "R_th", "Nu", "f_friction", "P_pump",
+            "COP", "Q_vol", "T_max_surface", "T_avg_surface", "delta_T_max", "sigma_T", "fluid_temp_rise",
+            "elapsed_s", "mlups"]
+    out_rows = []
+    for r in rows:
+        d = {c: (r[c].item() if hasattr(r[c], "item") else r[c]) for c in cols}
+        state = {"design_type": d["design_idx"], "feature_size": d["feature_size"], "spacing": d["spacing"],
+                 "buffer_size": 10}
+        mask = geometry.generate_mask(state)
+        d["mask_sha256"] = _sha(mask.astype(np.int32))
+        d["porosity_check"] = float(gd.compute_porosity(mask))
+        Dh, V, A = gd.compute_hydraulic_diameter(mask)
+        d["Dh_check"], d["V_fluid"], d["A_wetted"] = float(Dh), int(V), int(A)
+        out_rows.append(d)
+    (HERE / "parquet_rows.json").write_text(json.dumps(out_rows, indent=1, sort_keys=True))
+
+    # ---- designs: a grid of states per family plus every selected row
+    states = []
+    for t in range(6):
+        for fs in (1.5, 3.3, 5.0, 8.5):
+            for sp in (1.5, 2.7, 6.0):
+                states.append({"design_type": t, "feature_size": fs, "spacing": sp, "buffer_size": 10})
+    designs = []
+    for s in states:
+        m = geometry.generate_mask(s)
+        designs.append({"state": s, "shape": list(m.shape), "sha256": _sha(m.astype(np.int32)),
+                        "n_solid": int((m == 1).sum())})
+    heat = {}
+    for name, fn in geometry.HEAT_SOURCE_REGISTRY.items():
+        seeds = (0, 1, 7) if name == "gaussian_hotspots" else (0,)
+        for sd in seeds:
+            hm = fn(128, 128, seed=sd).astype(np.float32)
+            heat[f"{name}:{sd}"] = {"sha256": _sha(hm), "sum": float(hm.astype(np.float64).sum()),
+                                    "max": float(hm.max()), "probe": [float(hm[17, 33]), float(hm[64, 64]),
+                                                                      float(hm[101, 90])]}
+    (HERE / "designs.json").write_text(json.dumps({"masks": designs, "heat_maps": heat}, indent=1))
+
+    # ---- metrics: the reference function on seeded fields over three masks
+    mcases = []
+    for k, s in enumerate([{"design_type": 1, "feature_size": 3.3, "spacing": 2.7, "buffer_size": 10},
+                           {"design_type": 2, "feature_size": 2.5, "spacing": 4.0, "buffer_size": 10},
+                           {"design_type": 3, "feature_size": 6.0, "spacing": 3.0, "buffer_size": 10}]):
+        mask = geometry.generate_mask(s)
+        rho, u, T = synthetic_fields(100 + k, mask.shape)
+        params = {"tau_fluid": 0.53 + 0.01 * k, "u_inlet_val": 0.02 + 0.01 * k}
+        Dh, V, A = gd.compute_hydraulic_diameter(mask)
+        res = gd.compute_macroscopic_metrics({"u": u, "rho": rho, "T": T}, mask, params, Dh, A, Pr=7.0)
+        mcases.append({"state": s, "seed": 100 + k, "params": params, "Dh": float(Dh), "A_wetted": int(A),
+                       "V_fluid": int(V), "porosity": float(gd.compute_porosity(mask)),
+                       "pressure_drop_all": float(np.mean(rho[1]) - np.mean(rho[-2])) / 3.0,
+                       "metrics": {k2: float(v) for k2, v in res.items()}})
+    (HERE / "metrics.json").write_text(json.dumps(mcases, indent=1))
+    print(f"wrote {len(out_rows)} rows, {len(designs)} masks, {len(heat)} heat maps, {len(mcases)} metric cases")
+
+
+if __name__ == "__main__":
+    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))

@@ -1,0 +1,195 @@
+"""The fused coupled step (libxac.so lattice) against the oracle's restatement of src/simulation.py.
+
+FP32 parity is bit-exact on finite inputs: identical fields after any number of steps. The 16-bit
+storage forms are measured against the FP64 oracle with stated bounds."""
+import numpy as np
+import pytest
+import torch
+
+from oracle.ref import Ref
+from xadvcool_b200 import designs
+from xadvcool_b200.lattice import Lattice
+from xadvcool_b200.simulation import run_simulation
+
+pytestmark = pytest.mark.gpu
+
+C1 = dict(tau_fluid=0.6, heat_power=1e-4, u_inlet_val=0.05, Pr=2.0, k_ratio=100.0, t_inlet=25.0)
+
+
+def channel(seed, nx=24, ny=11, nz=9, solid_frac=0.15):
+    rng = np.random.default_rng(seed)
+    m = np.zeros((nx, ny, nz), np.int32)
+    m[rng.random((nx, ny, nz)) < solid_frac] = 1
+    m[:, 0, :] = 1
+    m[:, -1, :] = 1
+    m[:, :, :2] = 1
+    m[:, :, -1] = 1
+    m[0, 1:-1, 2:-1] = 2
+    m[-1, 1:-1, 2:-1] = 3
+    hs = np.zeros((nx, ny, nz), np.float32)
+    hs[:, :, 0] = rng.random((nx, ny)).astype(np.float32)
+    return m, hs
+
+
+def oracle_fields(mask, steps, hs=None, init=None, **kw):
+    return Ref(32).run_simulation(mask, max_steps=steps, tol_ke=0, tol_T=0, stats_every=10 ** 9, heat_source=hs,
+                                  init_fields=init, **kw)
+
+
+def lattice_fields(mask, steps, hs=None, chunks=None, **kw):
+    lat = Lattice(mask, heat_source=hs, **kw)
+    for n in (chunks or [steps]):
+        lat.step(n)
+    rho, u, T = (a.cpu().numpy() for a in lat.fields())
+    return lat, rho, u, T
+
+
+def assert_exact(ref, rho, u, T):
+    for name, a, b in (("rho", ref["rho"], rho), ("u", ref["u"], u), ("T", ref["T"], T)):
+        d = np.abs(a.astype(np.float64) - b.astype(np.float64))
+        assert np.array_equal(a, b), f"{name}: {np.count_nonzero(d)} cells differ, max |diff| {d.max():.3e}"
+
+
+def test_config1_straight_fin_plate_2000_steps_bit_exact(cuda):
+    mask = designs.straight_fin_plate()
+    ref = oracle_fields(mask, 2000, **C1)
+    _, rho, u, T = lattice_fields(mask, 2000, **C1)
+    assert_exact(ref, rho, u, T)
+    assert float(np.abs(u).max()) < 0.17
+
+
+@pytest.mark.parametrize("chunks", [[1], [2], [1, 1, 1], [7], [8], [3, 20, 1], [50]])
+def test_random_channel_step_chunking_bit_exact(chunks, cuda):
+    mask, hs = channel(11)
+    kw = dict(tau_fluid=0.57, heat_power=3e-3, u_inlet_val=0.04, Pr=3.0, k_ratio=30.0)
+    ref = oracle_fields(mask, sum(chunks), hs=hs, **kw)
+    _, rho, u, T = lattice_fields(mask, sum(chunks), hs=hs, chunks=chunks, **kw)
+    assert_exact(ref, rho, u, T)
+
+
+@pytest.mark.parametrize("shape", [(3, 3, 3), (5, 1, 1), (40, 3, 17), (17, 33, 5)])
+def test_ragged_and_tiny_lattices(shape, cuda):
+    rng = np.random.default_rng(sum(shape))
+    mask = rng.choice([0, 0, 1, 2, 3], size=shape).astype(np.int32)
+    kw = dict(tau_fluid=0.7, heat_power=1e-2, u_inlet_val=0.02, Pr=1.5, k_ratio=10.0)
+    ref = oracle_fields(mask, 25, **kw)
+    _, rho, u, T = lattice_fields(mask, 25, **kw)
+    assert_exact(ref, rho, u, T)
+
+
+def test_all_solid_and_all_fluid(cuda):
+    for fill in (0, 1):
+        mask = np.full((10, 6, 5), fill, np.int32)
+        ref = oracle_fields(mask, 12, tau_fluid=0.6, heat_power=0.1, u_inlet_val=0.03)
+        _, rho, u, T = lattice_fields(mask, 12, tau_fluid=0.6, heat_power=0.1, u_inlet_val=0.03)
+        assert_exact(ref, rho, u, T)
+
+
+def test_stats_match_oracle(cuda):
+    mask, hs = channel(12)
+    kw = dict(tau_fluid=0.6, heat_power=1e-3, u_inlet_val=0.05, Pr=2.0, k_ratio=20.0)
+    ref = oracle_fields(mask, 300, hs=hs, **kw)
+    lat, rho, u, T = lattice_fields(mask, 300, hs=hs, **kw)
+    s_c = Ref(32).stats(ref["rho"], ref["u"], ref["T"], mask)
+    assert np.allclose(s_c, lat.stats(), rtol=1e-12, atol=1e-14)
+
+
+def test_native_run_loop_matches_oracle_driver(cuda):
+    mask, hs = channel(13, nx=20)
+    kw = dict(tau_fluid=0.8, heat_power=1e-3, u_inlet_val=0.02, Pr=1.0, k_ratio=5.0)
+    ref = Ref(32).run_simulation(mask, max_steps=3000, tol_ke=1e-4, tol_T=1e-4, heat_source=hs, **kw)
+    out = run_simulation(mask, max_steps=3000, tol_ke=1e-4, tol_T=1e-4, heat_source=hs, silent=True, **kw)
+    assert out["steps"] == ref["steps"] and out["converged"] == ref["converged"]
+    assert_exact(ref, out["rho"], out["u"], out["T"])
+    assert out["d_ke"] == pytest.approx(ref["d_ke"], rel=1e-6, abs=1e-12)
+
+
+def test_divergence_guard(cuda):
+    mask, _ = channel(14, solid_frac=0.3)
+    out = run_simulation(mask, max_steps=4000, tau_fluid=0.52, u_inlet_val=0.3, tol_ke=0, tol_T=0, silent=True)
+    ref = Ref(32).run_simulation(mask, max_steps=4000, tau_fluid=0.52, u_inlet_val=0.3, tol_ke=0, tol_T=0)
+    assert ref["diverged"] and not out["converged"] and out["steps"] == ref["steps"] < 4000
+
+
+def test_nan_populations_are_reported_as_divergence(cuda):
+    mask, _ = channel(15)
+    lat = Lattice(mask, tau_fluid=0.6, u_inlet_val=0.03)
+    lat.step(3)
+    T = torch.full(mask.shape, float("nan"), device="cuda")
+    lat.init_fields(None, None, T)
+    lat.step(100)
+    st = lat.stats()
+    assert st[16] > 0
+    res = lat.run(max_steps=200, tol_ke=0, tol_T=0)
+    assert res["diverged"] and not res["converged"]
+
+
+def test_save_load_roundtrip(cuda):
+    mask, hs = channel(16)
+    kw = dict(tau_fluid=0.6, heat_power=1e-3, u_inlet_val=0.04, Pr=2.0, k_ratio=20.0, heat_source=hs)
+    lat = Lattice(mask, **kw)
+    lat.step(31)
+    blob = lat.save_state()
+    lat.step(20)
+    a = [t.cpu().numpy() for t in lat.fields()]
+    lat2 = Lattice(mask, **kw)
+    lat2.load_state(blob)
+    assert lat2.steps_done == 31
+    lat2.step(20)
+    b = [t.cpu().numpy() for t in lat2.fields()]
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+
+
+def test_warm_start_matches_oracle(cuda):
+    mask, hs = channel(17)
+    kw = dict(tau_fluid=0.6, heat_power=1e-3, u_inlet_val=0.04, Pr=2.0, k_ratio=20.0)
+    rng = np.random.default_rng(3)
+    rho0 = rng.uniform(0.98, 1.02, mask.shape).astype(np.float32)
+    u0 = rng.uniform(-0.02, 0.02, mask.shape + (3,)).astype(np.float32)
+    T0 = rng.uniform(25.0, 30.0, mask.shape).astype(np.float32)
+    solid = mask == 1
+    rho0[solid] = 1.0   # the warm start treats solid cells as at rest, like the cold start
+    u0[solid] = 0.0
+    ref = oracle_fields(mask, 40, hs=hs, init=(rho0, u0, T0), **kw)
+    lat = Lattice(mask, heat_source=hs, **kw)
+    lat.init_fields(*(torch.from_numpy(a).cuda() for a in (rho0, u0, T0)))
+    lat.step(40)
+    rho, u, T = (t.cpu().numpy() for t in lat.fields())
+    assert_exact(ref, rho, u, T)
+
+
+def test_two_runs_are_identical(cuda):
+    mask, hs, u_in, _ = designs.gyroid_design(0, nx=60, ny=40, nz=16)
+    a = [t.cpu().numpy() for t in lattice_fields(mask, 200, hs=hs, tau_fluid=0.55, u_inlet_val=u_in)[1:]]
+    b = [t.cpu().numpy() for t in lattice_fields(mask, 200, hs=hs, tau_fluid=0.55, u_inlet_val=u_in)[1:]]
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+
+
+def test_pump_constant_power_tracks_oracle(cuda):
+    mask, _ = channel(18, nx=30)
+    kw = dict(tau_fluid=0.6, heat_power=1e-3, u_inlet_val=0.03, Pr=2.0, k_ratio=20.0, pump_mode="constant_power",
+              target_power=0.05)
+    ref = Ref(32).run_simulation(mask, max_steps=2600, tol_ke=0, tol_T=0, **kw)
+    lat = Lattice(mask, **{k: v for k, v in kw.items() if k not in ("pump_mode", "target_power")})
+    res = lat.run(max_steps=2600, tol_ke=0, tol_T=0, pump_mode="constant_power", target_power=0.05)
+    assert res["u_inlet_final"] == pytest.approx(ref["u_inlet_final"], rel=1e-5)
+    assert res["u_inlet_final"] != pytest.approx(0.03, rel=1e-3)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp16", 2e-2), ("bf16", 1e-1)])
+def test_16bit_storage_error_vs_fp64_oracle(precision, tol, cuda):
+    mask = designs.straight_fin_plate()
+    ref64 = Ref(64).run_simulation(mask, max_steps=2000, tol_ke=0, tol_T=0, stats_every=10 ** 9, **C1)
+    _, rho, u, T = lattice_fields(mask, 2000, precision=precision, **C1)
+
+    def rel_l2(a, b):
+        return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+    fl = mask != 1
+    e_u = rel_l2(u[fl].astype(np.float64), ref64["u"][fl])
+    e_p = rel_l2(rho[fl].astype(np.float64) - 1.0, ref64["rho"][fl] - 1.0)
+    e_T = rel_l2(T.astype(np.float64) - 25.0, ref64["T"] - 25.0)
+    print(f"{precision}: rel L2 u {e_u:.3e} p {e_p:.3e} T {e_T:.3e}")
+    assert max(e_u, e_T) < tol

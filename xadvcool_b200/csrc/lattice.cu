@@ -1,0 +1,881 @@
+// Lattice object of libxac.so: owns the fused-step state of one design and implements the
+// xac_lattice_* entry points (the path of src/simulation.py:14-162).
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <utility>
+#include <vector>
+
+#include "lattice_kernels.cuh"
+#include "reductions.cuh"
+
+namespace xac {
+
+// ---------------------------------------------------------------- error plumbing
+namespace {
+thread_local char g_err[512] = "";
+}
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+int cuda_status(cudaError_t e, const char* what) {
+  set_error("%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+  return e == cudaErrorMemoryAllocation ? XAC_ENOMEM : XAC_ECUDA;
+}
+
+namespace {
+
+constexpr int kBlock = 256;
+
+// ---------------------------------------------------------------- layout / setup kernels
+// reference index r = (x*ny + y)*nz + z  <->  internal index c = (z*ny + y)*nx + x
+__device__ __forceinline__ long long ref_index(int x, int y, int z, int ny, int nz) {
+  return ((long long)x * ny + y) * nz + z;
+}
+
+__global__ void build_link_kernel(const uint8_t* __restrict__ type, const float* __restrict__ qsrc,
+                                  uint32_t* __restrict__ link, Geom g) {
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= g.ncell) return;
+  const int x = (int)(c % g.nx);
+  const long long t = c / g.nx;
+  const int y = (int)(t % g.ny), z = (int)(t / g.ny);
+  uint32_t w = 0;
+#pragma unroll
+  for (int i = 1; i < kQ; ++i) {
+    const int sx = x - ex_of(i), sy = y - ey_of(i), sz = z - ez_of(i);
+    bool bb = sx < 0 || sx >= g.nx || sy < 0 || sy >= g.ny || sz < 0 || sz >= g.nz;
+    if (!bb) bb = type[((long long)sz * g.ny + sy) * g.nx + sx] == kSolid;
+    if (bb) w |= 1u << i;
+  }
+  w |= (uint32_t)(type[c] & 3) << kTypeShift;
+  if (qsrc[c] > 0.0f) w |= kHeatedBit;
+  link[c] = w;
+}
+
+// ref-layout fields (any may be null = cold-start constant) -> internal rho, ux, uy, uz, T
+__global__ void import_fields_kernel(const float* __restrict__ rho_r, const float* __restrict__ u_r,
+                                     const float* __restrict__ T_r, const uint8_t* __restrict__ type, float T_cold,
+                                     float* __restrict__ rho, float* __restrict__ ux, float* __restrict__ uy,
+                                     float* __restrict__ uz, float* __restrict__ T, Geom g) {
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= g.ncell) return;
+  const int x = (int)(c % g.nx);
+  const long long t = c / g.nx;
+  const int y = (int)(t % g.ny), z = (int)(t / g.ny);
+  const long long r = ref_index(x, y, z, g.ny, g.nz);
+  const bool solid = type[c] == kSolid;
+  rho[c] = (rho_r && !solid) ? rho_r[r] : 1.0f;
+  ux[c] = (u_r && !solid) ? u_r[3 * r] : 0.0f;
+  uy[c] = (u_r && !solid) ? u_r[3 * r + 1] : 0.0f;
+  uz[c] = (u_r && !solid) ? u_r[3 * r + 2] : 0.0f;
+  T[c] = T_r ? T_r[r] : T_cold;
+}
+
+// simulation.py:89-90 (equilibria) followed by the fluid collision of the reference's first replay
+// (simulation.py:94), which this scheme performs ahead of the first streaming step.
+template <typename S>
+__global__ void init_state_kernel(const float* __restrict__ rho, const float* __restrict__ ux,
+                                  const float* __restrict__ uy, const float* __restrict__ uz,
+                                  const float* __restrict__ T, const uint8_t* __restrict__ type, S* __restrict__ P0,
+                                  S* __restrict__ P1, S* __restrict__ Q0, StepParams p) {
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= p.g.ncell) return;
+  const long long N = p.g.N;
+  const float r = rho[c], vx = ux[c], vy = uy[c], vz = uz[c];
+  const bool solid = type[c] == kSolid;
+  const float usq15 = 1.5f * ((vx * vx + vy * vy) + vz * vz);
+  const float omega = 1.0f / p.tau_f;
+  const float Tc = T[c];
+  const float tx = solid ? 0.0f : vx, ty = solid ? 0.0f : vy, tz = solid ? 0.0f : vz;
+  const float usq15t = 1.5f * ((tx * tx + ty * ty) + tz * tz);
+#define XAC_INIT(I)                                                                   \
+  {                                                                                   \
+    const float fe = feq_term(w_of(I) * r, edotu<I>(vx, vy, vz), usq15);             \
+    const float pc = solid ? fe : fe - omega * (fe - fe);                             \
+    Pop<S>::st(P0 + (long long)I * N + c, pc, w_of(I));                               \
+    Pop<S>::st(P1 + (long long)I * N + c, pc, w_of(I));                               \
+    const float ge = feq_term(w_of(I) * Tc, edotu<I>(tx, ty, tz), usq15t);           \
+    Pop<S>::st(Q0 + (long long)I * N + c, ge, w_of(I) * p.T_ref);                     \
+  }
+  XAC_FOR19(XAC_INIT)
+#undef XAC_INIT
+}
+
+// internal -> reference layout export
+__global__ void export_fields_kernel(const float* __restrict__ rho, const float* __restrict__ ux,
+                                     const float* __restrict__ uy, const float* __restrict__ uz,
+                                     const float* __restrict__ T, float* __restrict__ rho_r, float* __restrict__ u_r,
+                                     float* __restrict__ T_r, Geom g) {
+  const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (r >= g.ncell) return;
+  const int z = (int)(r % g.nz);
+  const long long t = r / g.nz;
+  const int y = (int)(t % g.ny), x = (int)(t / g.ny);
+  const long long c = ((long long)z * g.ny + y) * g.nx + x;
+  if (rho_r) rho_r[r] = rho[c];
+  if (u_r) {
+    u_r[3 * r] = ux[c];
+    u_r[3 * r + 1] = uy[c];
+    u_r[3 * r + 2] = uz[c];
+  }
+  if (T_r) T_r[r] = T[c];
+}
+
+__global__ void set_scalar_kernel(float* dst, float v) { *dst = v; }
+
+template <typename T>
+int dmalloc(T** p, size_t count, const char* what) {
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T) + 16);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return cuda_status(e, what);
+  }
+  return XAC_OK;
+}
+
+int reduction_blocks(long long n) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  long long want = (n + kBlock * 8 - 1) / (kBlock * 8);
+  long long cap = (long long)sms * 4;
+  if (want > cap) want = cap;
+  if (want < 1) want = 1;
+  return (int)want;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- the lattice object
+struct LatticeImpl {
+  Geom g{};
+  int precision = XAC_FP32;
+  size_t pop_elem = 4;
+  double tau_fluid = 0.6, Pr = 7.0, k_ratio = 628.0, u_inlet_nominal = 0.03, rho_outlet = 1.0, t_inlet = 25.0,
+         heat_power = 0.1;
+  float tau_th_f = 0.5f, tau_th_s = 0.5f;
+  float u_in_host = 0.0f;
+
+  void* P[2] = {nullptr, nullptr};
+  void* Qb[2] = {nullptr, nullptr};
+  int cur = 0;
+  uint8_t* type = nullptr;
+  uint32_t* link = nullptr;
+  float* qsrc = nullptr;
+  float* u_in = nullptr;
+  float *rho = nullptr, *ux = nullptr, *uy = nullptr, *uz = nullptr, *T = nullptr;
+  double* rows = nullptr;  // reduction partials
+  double* red_out = nullptr;
+  double* host_out = nullptr;  // pinned
+  int red_blocks = 1;
+  long long step = 0;
+  bool own_pending = true;    // next step reads the initial thermal populations unstreamed
+  long long macro_step = 0;   // rho/u arrays hold the fields of this step
+  long long T_step = 0;       // T array holds the field of this step
+  cudaStream_t capture = nullptr;
+  std::map<std::pair<int, int>, cudaGraphExec_t> graphs;  // (n, parity) -> n steps with macro output at the end
+  std::mutex mu;
+
+  StepParams params() const {
+    StepParams p;
+    p.g = g;
+    p.tau_f = (float)tau_fluid;
+    p.tau_tf = tau_th_f;
+    p.tau_ts = tau_th_s;
+    p.T_in = (float)t_inlet;
+    p.rho_out = (float)rho_outlet;
+    p.T_ref = precision == XAC_FP32 ? 0.0f : (float)t_inlet;
+    return p;
+  }
+
+  ~LatticeImpl() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    for (void* b : {P[0], P[1], Qb[0], Qb[1]}) cudaFree(b);
+    cudaFree(type);
+    cudaFree(link);
+    cudaFree(qsrc);
+    cudaFree(u_in);
+    cudaFree(rho);
+    cudaFree(ux);
+    cudaFree(uy);
+    cudaFree(uz);
+    cudaFree(T);
+    cudaFree(rows);
+    cudaFree(red_out);
+    if (host_out) cudaFreeHost(host_out);
+    if (capture) cudaStreamDestroy(capture);
+  }
+
+  template <typename S>
+  int launch_step(cudaStream_t s, bool macro, bool own) {
+    const StepParams p = params();
+    const S* Pin = (const S*)P[cur];
+    S* Pout = (S*)P[cur ^ 1];
+    const S* Qin = (const S*)Qb[cur];
+    S* Qout = (S*)Qb[cur ^ 1];
+    const unsigned grid = grid_for(g.ncell, kBlock);
+    if (macro && own)
+      coupled_step_kernel<S, true, true><<<grid, kBlock, 0, s>>>(Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux, uy,
+                                                                 uz, T, p);
+    else if (macro)
+      coupled_step_kernel<S, true, false><<<grid, kBlock, 0, s>>>(Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux, uy,
+                                                                  uz, T, p);
+    else if (own)
+      coupled_step_kernel<S, false, true><<<grid, kBlock, 0, s>>>(Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux,
+                                                                  uy, uz, T, p);
+    else
+      coupled_step_kernel<S, false, false><<<grid, kBlock, 0, s>>>(Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux,
+                                                                   uy, uz, T, p);
+    cur ^= 1;
+    return XAC_OK;
+  }
+
+  int launch_step_any(cudaStream_t s, bool macro, bool own) {
+    switch (precision) {
+      case XAC_FP16: return launch_step<__half>(s, macro, own);
+      case XAC_BF16: return launch_step<__nv_bfloat16>(s, macro, own);
+      default: return launch_step<float>(s, macro, own);
+    }
+  }
+
+  // n plain steps (no own step), the last one writing rho/u
+  int launch_plain(cudaStream_t s, int n) {
+    for (int k = 0; k < n; ++k) {
+      int r = launch_step_any(s, k == n - 1, false);
+      if (r != XAC_OK) return r;
+    }
+    return XAC_OK;
+  }
+
+  int steps(int n, cudaStream_t s) {
+    if (n <= 0) return XAC_OK;
+    if (own_pending) {
+      launch_step_any(s, n == 1, true);
+      own_pending = false;
+      step += 1;
+      --n;
+      XAC_CUDA(cudaGetLastError());
+    }
+    if (n > 0) {
+      if (n >= 8) {
+        auto key = std::make_pair(n, cur);
+        auto it = graphs.find(key);
+        if (it == graphs.end()) {
+          if (!capture) XAC_CUDA(cudaStreamCreateWithFlags(&capture, cudaStreamNonBlocking));
+          const int saved = cur;
+          cudaGraph_t graph = nullptr;
+          XAC_CUDA(cudaStreamBeginCapture(capture, cudaStreamCaptureModeThreadLocal));
+          launch_plain(capture, n);
+          cudaError_t e = cudaStreamEndCapture(capture, &graph);
+          cur = saved;
+          if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
+          cudaGraphExec_t exec = nullptr;
+          e = cudaGraphInstantiate(&exec, graph, 0);
+          cudaGraphDestroy(graph);
+          if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
+          it = graphs.emplace(key, exec).first;
+        }
+        XAC_CUDA(cudaGraphLaunch(it->second, s));
+        if (n & 1) cur ^= 1;
+      } else {
+        launch_plain(s, n);
+      }
+      step += n;
+      XAC_CUDA(cudaGetLastError());
+    }
+    macro_step = step;
+    return XAC_OK;
+  }
+
+  int finalize_T(cudaStream_t s) {
+    if (T_step == step) return XAC_OK;
+    const StepParams p = params();
+    const unsigned grid = grid_for(g.ncell, kBlock);
+    switch (precision) {
+      case XAC_FP16:
+        thermal_finalize_kernel<__half><<<grid, kBlock, 0, s>>>((const __half*)Qb[cur], link, T, p);
+        break;
+      case XAC_BF16:
+        thermal_finalize_kernel<__nv_bfloat16><<<grid, kBlock, 0, s>>>((const __nv_bfloat16*)Qb[cur], link, T, p);
+        break;
+      default:
+        thermal_finalize_kernel<float><<<grid, kBlock, 0, s>>>((const float*)Qb[cur], link, T, p);
+    }
+    XAC_CUDA(cudaGetLastError());
+    T_step = step;
+    return XAC_OK;
+  }
+
+  FieldView view() const {
+    FieldView v{};
+    v.rho = rho;
+    v.ux = ux;
+    v.uy = uy;
+    v.uz = uz;
+    v.ustride = 1;
+    v.T = T;
+    v.mask = nullptr;
+    v.link = link;
+    v.sx = 1;
+    v.sy = g.nx;
+    v.sz = (long long)g.nx * g.ny;
+    v.nx = g.nx;
+    v.ny = g.ny;
+    v.nz = g.nz;
+    return v;
+  }
+};
+
+// ---------------------------------------------------------------- shared reduction drivers
+int run_stats(const FieldView& v, double* rows, int nblocks, double* dev_out, double* host_out, cudaStream_t s) {
+  const auto spec = stats_spec();
+  stats_partials_kernel<<<nblocks, kBlock, 0, s>>>(v, spec, rows);
+  combine_rows_kernel<kNStats><<<1, 32, 0, s>>>(rows, nblocks, spec, dev_out);
+  XAC_CUDA(cudaGetLastError());
+  XAC_CUDA(cudaMemcpyAsync(host_out, dev_out, kNStats * sizeof(double), cudaMemcpyDeviceToHost, s));
+  XAC_CUDA(cudaStreamSynchronize(s));
+  return XAC_OK;
+}
+
+int run_metrics(const FieldView& v, MetricBox b, double* rows, int nblocks, double* dev_out, double* host_raw,
+                cudaStream_t s) {
+  const auto spec = metric_spec();
+  metric_partials_kernel<<<nblocks, kBlock, 0, s>>>(v, b, spec, rows);
+  combine_rows_kernel<kNMetrics><<<1, 32, 0, s>>>(rows, nblocks, spec, dev_out);
+  XAC_CUDA(cudaGetLastError());
+  XAC_CUDA(cudaMemcpyAsync(host_raw, dev_out, kNMetrics * sizeof(double), cudaMemcpyDeviceToHost, s));
+  XAC_CUDA(cudaStreamSynchronize(s));
+  return XAC_OK;
+}
+
+// generate_dataset.py:57-179 assembled from the FP64 partial sums.
+void assemble_scalars(const double* m, int nx, int ny, int nz, int buf, double t_inlet, double tau_fluid, double Pr,
+                      double u_inlet, double* out) {
+  for (int k = 0; k < XAC_NSCALARS; ++k) out[k] = 0.0;
+  const double Q_vol = m[kM_QVOL];
+  const double rho_in = m[kM_N_IN] > 0 ? m[kM_RHO_IN] / m[kM_N_IN] : 1.0;
+  const double rho_out = m[kM_N_OUT] > 0 ? m[kM_RHO_OUT] / m[kM_N_OUT] : 1.0;
+  const double dP = (rho_in - rho_out) / 3.0;
+  const double P_pump = std::fabs(dP * Q_vol);
+  const double ts_n = m[kM_TS_N] > 0 ? m[kM_TS_N] : 1.0;
+  const double Tmax_s = m[kM_TS_MAX], Tmin_s = m[kM_TS_MIN];
+  const double Tavg_s = m[kM_TS_SUM] / ts_n;
+  const double var = m[kM_TS_SQ] / ts_n - Tavg_s * Tavg_s;
+  const double sigma = std::sqrt(var > 0 ? var : 0.0);
+  const double total_flux = Q_vol;
+  const double Tout_avg = std::fabs(total_flux) > 1e-12 ? m[kM_QOUT] / total_flux : t_inlet;
+  const double Q_out_flux = m[kM_QOUT], Q_in_flux = t_inlet * total_flux;
+  const double dq = Q_out_flux - Q_in_flux;
+  const double Q_abs = std::fabs(dq) > 1e-12 ? std::fabs(dq) : 1e-12;
+  const double R_th = (Tmax_s - t_inlet) / Q_abs;
+  const double Tf_avg = m[kM_TF_N] > 0 ? m[kM_TF_SUM] / m[kM_TF_N] : t_inlet;
+  const double dT_conv = Tavg_s - Tf_avg;
+  const double V_fluid = m[kM_VFLUID], A_wet = m[kM_FACES];
+  const double Dh = A_wet > 0 ? 4.0 * V_fluid / A_wet : (double)ny;
+  const double h_avg = (std::fabs(dT_conv) > 1e-6 && A_wet > 0) ? Q_abs / (A_wet * std::fabs(dT_conv)) : 0.0;
+  const double tau_th_f = 0.5 + (tau_fluid - 0.5) / Pr;
+  const double k_f = (1.0 / 3.0) * (tau_th_f - 0.5);
+  const double Nu = k_f > 1e-12 ? h_avg * Dh / k_f : 0.0;
+  const double L = nx - 2 * buf;
+  const double rho_avg = (rho_in + rho_out) / 2.0;
+  const double f = u_inlet > 1e-12 ? (std::fabs(dP) * Dh) / (2.0 * L * rho_avg * u_inlet * u_inlet) : 0.0;
+  const double COP = P_pump > 1e-12 ? Q_abs / P_pump : 0.0;
+  out[XAC_SC_DP] = dP;
+  out[XAC_SC_RTH] = R_th;
+  out[XAC_SC_NU] = Nu;
+  out[XAC_SC_F_FRICTION] = f;
+  out[XAC_SC_P_PUMP] = P_pump;
+  out[XAC_SC_COP] = COP;
+  out[XAC_SC_Q_VOL] = Q_vol;
+  out[XAC_SC_T_MAX_SURFACE] = Tmax_s;
+  out[XAC_SC_T_AVG_SURFACE] = Tavg_s;
+  out[XAC_SC_DELTA_T_MAX] = Tmax_s - Tmin_s;
+  out[XAC_SC_SIGMA_T] = sigma;
+  out[XAC_SC_FLUID_TEMP_RISE] = Tout_avg - t_inlet;
+  const double plane = (double)ny * nz;
+  out[XAC_SC_PRESSURE_DROP_ALL] = (m[kM_RHO1_ALL] / plane - m[kM_RHO2_ALL] / plane) / 3.0;
+  out[XAC_SC_MAX_VELOCITY] = m[kM_MAXV];
+  out[XAC_SC_MAX_TEMPERATURE] = m[kM_MAXT];
+  out[XAC_SC_MEAN_TEMPERATURE] = m[kM_TSUM_ALL] / ((double)nx * ny * nz);
+  out[XAC_SC_DH] = Dh;
+  out[XAC_SC_V_FLUID] = V_fluid;
+  out[XAC_SC_A_WETTED] = A_wet;
+  const double core_size = (double)(nx - 2 * buf) * ny * nz;
+  out[XAC_SC_POROSITY] = core_size > 0 ? 1.0 - m[kM_CORE_SOLID] / core_size : 0.0;
+  out[XAC_SC_Q_ABSORBED] = Q_abs;
+  out[XAC_SC_DT_CONV] = dT_conv;
+  out[XAC_SC_RHO_AVG] = rho_avg;
+}
+
+}  // namespace xac
+
+struct xac_lattice {
+  xac::LatticeImpl impl;
+};
+
+using namespace xac;
+
+namespace {
+
+// Normalised heat source times power, internal layout; simulation.py:77-86 and thermal_engine3d.py:116-117.
+std::vector<float> host_qsrc(const xac_desc* d) {
+  const int nx = d->nx, ny = d->ny, nz = d->nz;
+  const size_t n = (size_t)nx * ny * nz;
+  std::vector<float> hs(n, 0.0f);
+  if (d->heat_source) {
+    std::memcpy(hs.data(), d->heat_source, n * sizeof(float));
+  } else {
+    for (int x = 0; x < nx; ++x)
+      for (int y = 0; y < ny; ++y) hs[((size_t)x * ny + y) * nz + 0] = 1.0f;
+  }
+  float mx = -INFINITY;
+  bool nan = false;
+  for (size_t i = 0; i < n; ++i) {
+    if (std::isnan(hs[i])) nan = true;
+    if (hs[i] > mx) mx = hs[i];
+  }
+  if (!nan && mx > 0.0f)
+    for (size_t i = 0; i < n; ++i) hs[i] = hs[i] / mx;
+  const float power = (float)d->heat_power;
+  std::vector<float> q(n);
+  for (int x = 0; x < nx; ++x)
+    for (int y = 0; y < ny; ++y)
+      for (int z = 0; z < nz; ++z)
+        q[((size_t)z * ny + y) * nx + x] = hs[((size_t)x * ny + y) * nz + z] * power;
+  return q;
+}
+
+int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
+  XAC_REQUIRE(d, "xac_lattice_create: null descriptor");
+  XAC_REQUIRE(d->nx >= 3 && d->ny >= 1 && d->nz >= 1, "xac_lattice_create: lattice %d x %d x %d too small", d->nx,
+              d->ny, d->nz);
+  XAC_REQUIRE((long long)d->nx * d->ny * d->nz < (1LL << 31), "xac_lattice_create: lattice too large");
+  XAC_REQUIRE(d->mask, "xac_lattice_create: null mask");
+  XAC_REQUIRE(d->tau_fluid > 0.5, "xac_lattice_create: tau_fluid must exceed 0.5 (got %g)", d->tau_fluid);
+  XAC_REQUIRE(d->Pr > 0, "xac_lattice_create: Pr must be positive");
+  XAC_REQUIRE(d->precision == XAC_FP32 || d->precision == XAC_FP16 || d->precision == XAC_BF16,
+              "xac_lattice_create: unknown precision %d", d->precision);
+  const int nx = d->nx, ny = d->ny, nz = d->nz;
+  const long long n = (long long)nx * ny * nz;
+  L.g.nx = nx;
+  L.g.ny = ny;
+  L.g.nz = nz;
+  L.g.ncell = n;
+  L.g.N = (n + 63) / 64 * 64;
+  L.precision = d->precision;
+  L.pop_elem = d->precision == XAC_FP32 ? 4 : 2;
+  L.tau_fluid = d->tau_fluid;
+  L.Pr = d->Pr;
+  L.k_ratio = d->k_ratio;
+  L.u_inlet_nominal = d->u_inlet;
+  L.rho_outlet = d->rho_outlet;
+  L.t_inlet = d->t_inlet;
+  L.heat_power = d->heat_power;
+  // simulation.py:70-71 in double, handed to the kernels as float32 like Warp's float parameters
+  const double tth_f = 0.5 + ((d->tau_fluid - 0.5) / d->Pr);
+  const double tth_s = 0.5 + d->k_ratio * (tth_f - 0.5);
+  L.tau_th_f = (float)tth_f;
+  L.tau_th_s = (float)tth_s;
+  L.u_in_host = (float)d->u_inlet;
+
+  std::vector<uint8_t> type(n);
+  for (int x = 0; x < nx; ++x)
+    for (int y = 0; y < ny; ++y)
+      for (int z = 0; z < nz; ++z) {
+        const int32_t m = d->mask[((size_t)x * ny + y) * nz + z];
+        XAC_REQUIRE(m >= 0 && m <= 3, "xac_lattice_create: mask value %d at (%d,%d,%d) is not a BC label", (int)m, x, y,
+                    z);
+        type[((size_t)z * ny + y) * nx + x] = (uint8_t)m;
+      }
+  std::vector<float> q = host_qsrc(d);
+
+  const size_t pop_bytes = (size_t)kQ * L.g.N * L.pop_elem;
+  for (int b = 0; b < 2; ++b) {
+    XAC_CUDA(cudaMalloc(&L.P[b], pop_bytes));
+    XAC_CUDA(cudaMalloc(&L.Qb[b], pop_bytes));
+  }
+  int r;
+  if ((r = dmalloc(&L.type, n, "alloc type")) != XAC_OK) return r;
+  if ((r = dmalloc(&L.link, n, "alloc link")) != XAC_OK) return r;
+  if ((r = dmalloc(&L.qsrc, n, "alloc qsrc")) != XAC_OK) return r;
+  if ((r = dmalloc(&L.u_in, 1, "alloc u_in")) != XAC_OK) return r;
+  for (float** f : {&L.rho, &L.ux, &L.uy, &L.uz, &L.T})
+    if ((r = dmalloc(f, n, "alloc fields")) != XAC_OK) return r;
+  L.red_blocks = reduction_blocks(n);
+  if ((r = dmalloc(&L.rows, (size_t)L.red_blocks * (kNMetrics > kNStats ? kNMetrics : kNStats), "alloc rows")) !=
+      XAC_OK)
+    return r;
+  if ((r = dmalloc(&L.red_out, 64, "alloc red_out")) != XAC_OK) return r;
+  XAC_CUDA(cudaMallocHost(&L.host_out, 64 * sizeof(double)));
+  // the pop planes' padding is never read, but keep it defined
+  for (int b = 0; b < 2; ++b) {
+    XAC_CUDA(cudaMemsetAsync(L.P[b], 0, pop_bytes, s));
+    XAC_CUDA(cudaMemsetAsync(L.Qb[b], 0, pop_bytes, s));
+  }
+  XAC_CUDA(cudaMemcpyAsync(L.type, type.data(), n, cudaMemcpyHostToDevice, s));
+  XAC_CUDA(cudaMemcpyAsync(L.qsrc, q.data(), n * sizeof(float), cudaMemcpyHostToDevice, s));
+  set_scalar_kernel<<<1, 1, 0, s>>>(L.u_in, L.u_in_host);
+  build_link_kernel<<<grid_for(n, kBlock), kBlock, 0, s>>>(L.type, L.qsrc, L.link, L.g);
+  XAC_CUDA(cudaGetLastError());
+  // host vectors go out of scope: make the copies complete first
+  XAC_CUDA(cudaStreamSynchronize(s));
+  return XAC_OK;
+}
+
+int init_impl(LatticeImpl& L, const float* rho, const float* u, const float* T, cudaStream_t s) {
+  const unsigned grid = grid_for(L.g.ncell, kBlock);
+  import_fields_kernel<<<grid, kBlock, 0, s>>>(rho, u, T, L.type, (float)L.t_inlet, L.rho, L.ux, L.uy, L.uz, L.T,
+                                               L.g);
+  const StepParams p = L.params();
+  switch (L.precision) {
+    case XAC_FP16:
+      init_state_kernel<__half><<<grid, kBlock, 0, s>>>(L.rho, L.ux, L.uy, L.uz, L.T, L.type, (__half*)L.P[0],
+                                                        (__half*)L.P[1], (__half*)L.Qb[0], p);
+      break;
+    case XAC_BF16:
+      init_state_kernel<__nv_bfloat16><<<grid, kBlock, 0, s>>>(L.rho, L.ux, L.uy, L.uz, L.T, L.type,
+                                                               (__nv_bfloat16*)L.P[0], (__nv_bfloat16*)L.P[1],
+                                                               (__nv_bfloat16*)L.Qb[0], p);
+      break;
+    default:
+      init_state_kernel<float><<<grid, kBlock, 0, s>>>(L.rho, L.ux, L.uy, L.uz, L.T, L.type, (float*)L.P[0],
+                                                       (float*)L.P[1], (float*)L.Qb[0], p);
+  }
+  XAC_CUDA(cudaGetLastError());
+  L.cur = 0;
+  L.step = 0;
+  L.own_pending = true;
+  L.macro_step = 0;
+  L.T_step = 0;
+  return XAC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* xac_last_error(void) { return xac::g_err; }
+int xac_version(void) { return 10000; }
+
+int xac_lattice_create(const xac_desc* desc, xac_lattice** out, void* stream) {
+  XAC_REQUIRE(out, "xac_lattice_create: null output handle");
+  *out = nullptr;
+  xac_lattice* lat = new (std::nothrow) xac_lattice();
+  if (!lat) {
+    set_error("xac_lattice_create: host allocation failed");
+    return XAC_ENOMEM;
+  }
+  cudaStream_t s = as_stream(stream);
+  int r = create_impl(desc, lat->impl, s);
+  if (r == XAC_OK) r = init_impl(lat->impl, nullptr, nullptr, nullptr, s);
+  if (r != XAC_OK) {
+    delete lat;
+    return r;
+  }
+  *out = lat;
+  return XAC_OK;
+}
+
+int xac_lattice_destroy(xac_lattice* lat) {
+  if (!lat) return XAC_OK;
+  cudaDeviceSynchronize();
+  delete lat;
+  return XAC_OK;
+}
+
+int xac_lattice_init_fields(xac_lattice* lat, const float* rho, const float* u, const float* T, void* stream) {
+  XAC_REQUIRE(lat, "xac_lattice_init_fields: null lattice");
+  std::lock_guard<std::mutex> g(lat->impl.mu);
+  return init_impl(lat->impl, rho, u, T, as_stream(stream));
+}
+
+int xac_lattice_step(xac_lattice* lat, int n, void* stream) {
+  XAC_REQUIRE(lat, "xac_lattice_step: null lattice");
+  XAC_REQUIRE(n >= 0, "xac_lattice_step: negative step count %d", n);
+  std::lock_guard<std::mutex> g(lat->impl.mu);
+  return lat->impl.steps(n, as_stream(stream));
+}
+
+int xac_lattice_stats(xac_lattice* lat, double* out_host, void* stream) {
+  XAC_REQUIRE(lat && out_host, "xac_lattice_stats: null pointer");
+  LatticeImpl& L = lat->impl;
+  std::lock_guard<std::mutex> g(L.mu);
+  cudaStream_t s = as_stream(stream);
+  int r = L.finalize_T(s);
+  if (r != XAC_OK) return r;
+  r = run_stats(L.view(), L.rows, L.red_blocks, L.red_out, L.host_out, s);
+  if (r != XAC_OK) return r;
+  std::memcpy(out_host, L.host_out, kNStats * sizeof(double));
+  return XAC_OK;
+}
+
+int xac_lattice_fields(xac_lattice* lat, float* rho, float* u, float* T, void* stream) {
+  XAC_REQUIRE(lat, "xac_lattice_fields: null lattice");
+  LatticeImpl& L = lat->impl;
+  std::lock_guard<std::mutex> g(L.mu);
+  cudaStream_t s = as_stream(stream);
+  if (T) {
+    int r = L.finalize_T(s);
+    if (r != XAC_OK) return r;
+  }
+  export_fields_kernel<<<grid_for(L.g.ncell, kBlock), kBlock, 0, s>>>(L.rho, L.ux, L.uy, L.uz, L.T, rho, u, T, L.g);
+  XAC_CUDA(cudaGetLastError());
+  return XAC_OK;
+}
+
+int xac_lattice_set_inlet(xac_lattice* lat, double u_inlet, void* stream) {
+  XAC_REQUIRE(lat, "xac_lattice_set_inlet: null lattice");
+  XAC_REQUIRE(std::isfinite(u_inlet) && u_inlet < 1.0, "xac_lattice_set_inlet: u_inlet %g out of range", u_inlet);
+  lat->impl.u_in_host = (float)u_inlet;
+  set_scalar_kernel<<<1, 1, 0, as_stream(stream)>>>(lat->impl.u_in, (float)u_inlet);
+  XAC_CUDA(cudaGetLastError());
+  return XAC_OK;
+}
+
+int xac_lattice_get_inlet(xac_lattice* lat, double* u_inlet, void*) {
+  XAC_REQUIRE(lat && u_inlet, "xac_lattice_get_inlet: null pointer");
+  *u_inlet = (double)lat->impl.u_in_host;
+  return XAC_OK;
+}
+
+int xac_lattice_steps_done(const xac_lattice* lat, long long* steps) {
+  XAC_REQUIRE(lat && steps, "xac_lattice_steps_done: null pointer");
+  *steps = lat->impl.step;
+  return XAC_OK;
+}
+
+int xac_lattice_scalars(xac_lattice* lat, const xac_scalar_params* prm, double* out_host, void* stream) {
+  XAC_REQUIRE(lat && prm && out_host, "xac_lattice_scalars: null pointer");
+  LatticeImpl& L = lat->impl;
+  XAC_REQUIRE(prm->buf >= 0 && 2 * prm->buf < L.g.nx, "xac_lattice_scalars: bad buffer length %d", prm->buf);
+  std::lock_guard<std::mutex> g(L.mu);
+  cudaStream_t s = as_stream(stream);
+  int r = L.finalize_T(s);
+  if (r != XAC_OK) return r;
+  MetricBox b{prm->buf, prm->core_nx, prm->core_ny};
+  r = run_metrics(L.view(), b, L.rows, L.red_blocks, L.red_out, L.host_out, s);
+  if (r != XAC_OK) return r;
+  assemble_scalars(L.host_out, L.g.nx, L.g.ny, L.g.nz, prm->buf, prm->t_inlet, prm->tau_fluid, prm->Pr,
+                   prm->u_inlet, out_host);
+  return XAC_OK;
+}
+
+int xac_lattice_state_bytes(const xac_lattice* lat, size_t* bytes) {
+  XAC_REQUIRE(lat && bytes, "xac_lattice_state_bytes: null pointer");
+  const LatticeImpl& L = lat->impl;
+  const size_t pop = (size_t)kQ * L.g.N * L.pop_elem;
+  *bytes = 64 + 2 * pop + 5 * (size_t)L.g.ncell * sizeof(float);
+  return XAC_OK;
+}
+
+int xac_lattice_save_state(xac_lattice* lat, void* host_dst, size_t bytes, void* stream) {
+  XAC_REQUIRE(lat && host_dst, "xac_lattice_save_state: null pointer");
+  size_t need = 0;
+  xac_lattice_state_bytes(lat, &need);
+  XAC_REQUIRE(bytes >= need, "xac_lattice_save_state: buffer of %zu bytes, need %zu", bytes, need);
+  LatticeImpl& L = lat->impl;
+  std::lock_guard<std::mutex> g(L.mu);
+  cudaStream_t s = as_stream(stream);
+  int r = L.finalize_T(s);
+  if (r != XAC_OK) return r;
+  int64_t hdr[8] = {0x58414331, L.g.nx, L.g.ny, L.g.nz, L.precision, L.step, L.own_pending ? 1 : 0, 0};
+  float u_in = L.u_in_host;
+  std::memcpy(&hdr[7], &u_in, sizeof(float));
+  char* dst = (char*)host_dst;
+  std::memcpy(dst, hdr, 64);
+  const size_t pop = (size_t)kQ * L.g.N * L.pop_elem;
+  const size_t nf = (size_t)L.g.ncell * sizeof(float);
+  XAC_CUDA(cudaMemcpyAsync(dst + 64, L.P[L.cur], pop, cudaMemcpyDeviceToHost, s));
+  XAC_CUDA(cudaMemcpyAsync(dst + 64 + pop, L.Qb[L.cur], pop, cudaMemcpyDeviceToHost, s));
+  const float* f[5] = {L.rho, L.ux, L.uy, L.uz, L.T};
+  for (int k = 0; k < 5; ++k)
+    XAC_CUDA(cudaMemcpyAsync(dst + 64 + 2 * pop + k * nf, f[k], nf, cudaMemcpyDeviceToHost, s));
+  XAC_CUDA(cudaStreamSynchronize(s));
+  return XAC_OK;
+}
+
+int xac_lattice_load_state(xac_lattice* lat, const void* host_src, size_t bytes, void* stream) {
+  XAC_REQUIRE(lat && host_src, "xac_lattice_load_state: null pointer");
+  size_t need = 0;
+  xac_lattice_state_bytes(lat, &need);
+  XAC_REQUIRE(bytes >= need, "xac_lattice_load_state: buffer of %zu bytes, need %zu", bytes, need);
+  LatticeImpl& L = lat->impl;
+  int64_t hdr[8];
+  std::memcpy(hdr, host_src, 64);
+  XAC_REQUIRE(hdr[0] == 0x58414331 && hdr[1] == L.g.nx && hdr[2] == L.g.ny && hdr[3] == L.g.nz &&
+                  hdr[4] == L.precision,
+              "xac_lattice_load_state: state was saved from a different lattice");
+  std::lock_guard<std::mutex> g(L.mu);
+  cudaStream_t s = as_stream(stream);
+  const char* src = (const char*)host_src;
+  const size_t pop = (size_t)kQ * L.g.N * L.pop_elem;
+  const size_t nf = (size_t)L.g.ncell * sizeof(float);
+  // solid cells are read from either buffer, so both get the saved fluid populations
+  XAC_CUDA(cudaMemcpyAsync(L.P[0], src + 64, pop, cudaMemcpyHostToDevice, s));
+  XAC_CUDA(cudaMemcpyAsync(L.P[1], src + 64, pop, cudaMemcpyHostToDevice, s));
+  XAC_CUDA(cudaMemcpyAsync(L.Qb[0], src + 64 + pop, pop, cudaMemcpyHostToDevice, s));
+  float* f[5] = {L.rho, L.ux, L.uy, L.uz, L.T};
+  for (int k = 0; k < 5; ++k)
+    XAC_CUDA(cudaMemcpyAsync(f[k], src + 64 + 2 * pop + k * nf, nf, cudaMemcpyHostToDevice, s));
+  float u_in;
+  std::memcpy(&u_in, &hdr[7], sizeof(float));
+  L.u_in_host = u_in;
+  set_scalar_kernel<<<1, 1, 0, s>>>(L.u_in, u_in);
+  XAC_CUDA(cudaStreamSynchronize(s));
+  L.cur = 0;
+  L.step = hdr[5];
+  L.own_pending = hdr[6] != 0;
+  L.macro_step = L.step;
+  L.T_step = L.step;
+  return XAC_OK;
+}
+
+// simulation.py:102-162
+int xac_lattice_run(xac_lattice* lat, const xac_run_opts* o, xac_run_result* res, void* stream) {
+  XAC_REQUIRE(lat && o && res, "xac_lattice_run: null pointer");
+  XAC_REQUIRE(o->stats_every > 0 && o->max_steps >= 0, "xac_lattice_run: bad options");
+  LatticeImpl& L = lat->impl;
+  std::memset(res, 0, sizeof(*res));
+  const int a = (int)(0.6 * o->max_steps);
+  const double mu = L.u_inlet_nominal > 1e-6 ? L.u_inlet_nominal : 1e-6;
+  int b = (int)(2.0 * L.g.nx / mu);
+  if (b < 5000) b = 5000;
+  const long long min_steps = a < b ? a : b;
+  double prev_ke = 0.0, prev_max_T = 0.0, d_ke = 0.0, dT = 0.0, prev_Q = 0.0, dQ = 1.0;
+  double st[kNStats];
+  const long long start = L.step;
+  long long step = 0;
+  int diverged = 0;
+  while (step < o->max_steps) {
+    int chunk = o->stats_every - (int)((start + step) % o->stats_every);
+    if (step + chunk > o->max_steps) chunk = (int)(o->max_steps - step);
+    int r = xac_lattice_step(lat, chunk, stream);
+    if (r != XAC_OK) return r;
+    step += chunk;
+    if ((start + step) % o->stats_every != 0) continue;
+    r = xac_lattice_stats(lat, st, stream);
+    if (r != XAC_OK) return r;
+    const double max_v = st[XAC_ST_MAX_V], ke = st[XAC_ST_SUM_KE], max_T = st[XAC_ST_MAX_T],
+                 Q_out = st[XAC_ST_Q_OUT];
+    const bool past = (start + step) > o->stats_every;
+    d_ke = past ? std::fabs(ke - prev_ke) / (prev_ke + 1e-9) / o->stats_every : 0.0;
+    dT = past ? std::fabs(max_T - prev_max_T) / (prev_max_T + 1e-9) / o->stats_every : 0.0;
+    dQ = past ? std::fabs(Q_out - prev_Q) / (std::fabs(prev_Q) + 1e-12) / o->stats_every : 1.0;
+    prev_ke = ke;
+    prev_max_T = max_T;
+    prev_Q = Q_out;
+    if (o->constant_power && (start + step) > 2000) {
+      double ue = (double)L.u_in_host;
+      const double rin = st[XAC_ST_C_IN] > 0 ? st[XAC_ST_SUM_RHO_IN] / st[XAC_ST_C_IN] : 1.0;
+      const double rout = st[XAC_ST_C_OUT] > 0 ? st[XAC_ST_SUM_RHO_OUT] / st[XAC_ST_C_OUT] : 1.0;
+      const double dP = (rin - rout) / 3.0;
+      const double pw = dP * (ue * st[XAC_ST_C_IN]);
+      ue = ue + 0.005 * (o->target_power - pw);
+      ue = ue < 0.0001 ? 0.0001 : (ue > 0.15 ? 0.15 : ue);
+      r = xac_lattice_set_inlet(lat, ue, stream);
+      if (r != XAC_OK) return r;
+    }
+    std::memcpy(res->last_stats, st, sizeof(st));
+    if (step > min_steps && d_ke < o->tol_ke && dT < o->tol_T && dQ < o->tol_T) break;
+    if (st[XAC_ST_NONFINITE] > 0 || max_v > 0.17 || max_T > 1e4) {
+      diverged = 1;
+      break;
+    }
+  }
+  res->steps = step;
+  res->converged = (step > min_steps && d_ke < o->tol_ke && dT < o->tol_T && dQ < o->tol_T) ? 1 : 0;
+  res->diverged = diverged;
+  res->d_ke = d_ke;
+  res->dT_conv = dT;
+  res->dQ_conv = dQ;
+  res->u_inlet_final = (double)L.u_in_host;
+  return XAC_OK;
+}
+
+// Deterministic stats of arbitrary reference-layout fields (the two reference stats kernels, merged).
+int xac_stats_fields(const float* rho, const float* u, const float* T, const int32_t* mask, int nx, int ny, int nz,
+                     double* out_host, void* stream) {
+  XAC_REQUIRE(rho && u && T && mask && out_host, "xac_stats_fields: null pointer");
+  XAC_REQUIRE(nx > 0 && ny > 0 && nz > 0, "xac_stats_fields: bad dimensions");
+  cudaStream_t s = as_stream(stream);
+  const long long n = (long long)nx * ny * nz;
+  const int nb = reduction_blocks(n);
+  double* rows = nullptr;
+  double* dout = nullptr;
+  double* hout = nullptr;
+  int r = dmalloc(&rows, (size_t)nb * kNStats, "alloc rows");
+  if (r == XAC_OK) r = dmalloc(&dout, kNStats, "alloc out");
+  if (r == XAC_OK && cudaMallocHost(&hout, kNStats * sizeof(double)) != cudaSuccess) r = XAC_ENOMEM;
+  if (r == XAC_OK) {
+    FieldView v{};
+    v.rho = rho;
+    v.ux = u;
+    v.uy = u + 1;
+    v.uz = u + 2;
+    v.ustride = 3;
+    v.T = T;
+    v.mask = mask;
+    v.link = nullptr;
+    v.sx = (long long)ny * nz;
+    v.sy = nz;
+    v.sz = 1;
+    v.nx = nx;
+    v.ny = ny;
+    v.nz = nz;
+    r = run_stats(v, rows, nb, dout, hout, s);
+    if (r == XAC_OK) std::memcpy(out_host, hout, kNStats * sizeof(double));
+  }
+  cudaFree(rows);
+  cudaFree(dout);
+  if (hout) cudaFreeHost(hout);
+  return r;
+}
+
+int xac_scalars_fields(const float* rho, const float* u, const float* T, const int32_t* mask, int nx, int ny, int nz,
+                       const xac_scalar_params* prm, double* out_host, void* stream) {
+  XAC_REQUIRE(rho && u && T && mask && prm && out_host, "xac_scalars_fields: null pointer");
+  XAC_REQUIRE(nx > 0 && ny > 0 && nz > 0, "xac_scalars_fields: bad dimensions");
+  XAC_REQUIRE(prm->buf >= 0 && 2 * prm->buf < nx, "xac_scalars_fields: bad buffer length %d", prm->buf);
+  cudaStream_t s = as_stream(stream);
+  const long long n = (long long)nx * ny * nz;
+  const int nb = reduction_blocks(n);
+  double* rows = nullptr;
+  double* dout = nullptr;
+  double* hout = nullptr;
+  int r = dmalloc(&rows, (size_t)nb * kNMetrics, "alloc rows");
+  if (r == XAC_OK) r = dmalloc(&dout, kNMetrics, "alloc out");
+  if (r == XAC_OK && cudaMallocHost(&hout, kNMetrics * sizeof(double)) != cudaSuccess) r = XAC_ENOMEM;
+  if (r == XAC_OK) {
+    FieldView v{};
+    v.rho = rho;
+    v.ux = u;
+    v.uy = u + 1;
+    v.uz = u + 2;
+    v.ustride = 3;
+    v.T = T;
+    v.mask = mask;
+    v.link = nullptr;
+    v.sx = (long long)ny * nz;
+    v.sy = nz;
+    v.sz = 1;
+    v.nx = nx;
+    v.ny = ny;
+    v.nz = nz;
+    MetricBox b{prm->buf, prm->core_nx, prm->core_ny};
+    r = run_metrics(v, b, rows, nb, dout, hout, s);
+    if (r == XAC_OK)
+      assemble_scalars(hout, nx, ny, nz, prm->buf, prm->t_inlet, prm->tau_fluid, prm->Pr, prm->u_inlet, out_host);
+  }
+  cudaFree(rows);
+  cudaFree(dout);
+  if (hout) cudaFreeHost(hout);
+  return r;
+}
+
+}  // extern "C"

@@ -1,0 +1,238 @@
+// Deterministic FP64 reductions over a 3-D field view: the stats of src/fluid_engine3d.py:277-312 and
+// src/thermal_engine3d.py:226-243 (which the reference accumulates with float atomics in no fixed order)
+// and the scalar metrics of generate_dataset.py:57-179. Each block reduces its cells with warp shuffles
+// into one row of partials; a single-block pass combines the rows in block order.
+#pragma once
+
+#include "lattice_kernels.cuh"
+
+namespace xac {
+
+// A read-only view of rho, u, T and the cell labels in either layout.
+struct FieldView {
+  const float* rho;
+  const float* ux;
+  const float* uy;
+  const float* uz;
+  int ustride;  // element stride between cells of one u component (3 = AoS vec3, 1 = SoA)
+  const float* T;
+  const int32_t* mask;   // reference labels, or
+  const uint32_t* link;  // packed link words (internal layout)
+  long long sx, sy, sz;  // element strides of the scalar fields along x, y, z
+  int nx, ny, nz;
+};
+
+__device__ __forceinline__ int view_type(const FieldView& v, long long cell) {
+  return v.mask ? (int)v.mask[cell] : link_type(v.link[cell]);
+}
+
+enum ReduceOp : int { kSum = 0, kMax = 1, kMin = 2 };
+
+template <int K>
+struct ReduceSpec {
+  int op[K];
+};
+
+__device__ __forceinline__ double combine(int op, double a, double b) {
+  return op == kSum ? a + b : (op == kMax ? fmax(a, b) : fmin(a, b));
+}
+__device__ __forceinline__ double identity(int op) {
+  return op == kSum ? 0.0 : (op == kMax ? -INFINITY : INFINITY);
+}
+
+// Block-level reduction of K values per thread; thread 0 writes out[0..K).
+template <int K>
+__device__ __forceinline__ void block_reduce(double (&acc)[K], const ReduceSpec<K>& spec, double* out) {
+  __shared__ double sm[32][K];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    double v = acc[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = combine(spec.op[k], v, __shfl_down_sync(0xffffffffu, v, o));
+    if (lane == 0) sm[warp][k] = v;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double v = lane < nw ? sm[lane][k] : identity(spec.op[k]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v = combine(spec.op[k], v, __shfl_down_sync(0xffffffffu, v, o));
+      if (lane == 0) out[k] = v;
+    }
+  }
+}
+
+// Combine nrows rows of K partials in row order (deterministic); one block, thread k owns column k.
+template <int K>
+__global__ void combine_rows_kernel(const double* __restrict__ rows, int nrows, ReduceSpec<K> spec,
+                                    double* __restrict__ out) {
+  const int k = threadIdx.x;
+  if (k >= K) return;
+  double v = identity(spec.op[k]);
+  for (int r = 0; r < nrows; ++r) v = combine(spec.op[k], v, rows[(long long)r * K + k]);
+  out[k] = v;
+}
+
+// ---- convergence / divergence stats (XAC_ST_* order) --------------------------------------------
+constexpr int kNStats = XAC_NSTATS;
+
+inline ReduceSpec<kNStats> stats_spec() {
+  ReduceSpec<kNStats> s{};
+  for (int k = 0; k < kNStats; ++k) s.op[k] = kSum;
+  s.op[XAC_ST_MAX_V] = kMax;
+  s.op[XAC_ST_MAX_T] = kMax;
+  return s;
+}
+
+__global__ void __launch_bounds__(256) stats_partials_kernel(FieldView v, ReduceSpec<kNStats> spec,
+                                                             double* __restrict__ rows) {
+  double acc[kNStats];
+#pragma unroll
+  for (int k = 0; k < kNStats; ++k) acc[k] = identity(spec.op[k]);
+  const long long n = (long long)v.nx * v.ny * v.nz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    // i enumerates cells x fastest; any order gives the same sums up to FP64 rounding
+    const int x = (int)(i % v.nx);
+    const long long t = i / v.nx;
+    const int y = (int)(t % v.ny), z = (int)(t / v.ny);
+    const long long cell = x * v.sx + y * v.sy + z * v.sz;
+    const int m = view_type(v, cell);
+    const float ux = v.ux[cell * v.ustride], uy = v.uy[cell * v.ustride], uz = v.uz[cell * v.ustride];
+    const float vsq = (ux * ux + uy * uy) + uz * uz;
+    const float vmag = sqrtf(vsq);
+    const float r = v.rho[cell], T = v.T[cell];
+    if (!isfinite(vmag) || !isfinite(T)) acc[XAC_ST_NONFINITE] += 1.0;
+    acc[XAC_ST_SUM_KE] += (double)vsq;
+    if (m != kSolid) {
+      acc[XAC_ST_MAX_V] = fmax(acc[XAC_ST_MAX_V], (double)vmag);
+      acc[XAC_ST_SUM_V] += (double)vmag;
+      acc[XAC_ST_COUNT] += 1.0;
+      acc[XAC_ST_SUM_RHO] += (double)r;
+    }
+    if (x == 1) {
+      acc[XAC_ST_SUM_RHO_IN] += (double)r;
+      acc[XAC_ST_C_IN] += 1.0;
+    }
+    if (x == v.nx - 2) {
+      acc[XAC_ST_SUM_RHO_OUT] += (double)r;
+      acc[XAC_ST_C_OUT] += 1.0;
+    }
+    if (m == kOutlet) {
+      acc[XAC_ST_SUM_UX_OUT] += (double)ux;
+      acc[XAC_ST_C_OUTLET] += 1.0;
+      acc[XAC_ST_Q_OUT] += (double)(ux * T);
+      acc[XAC_ST_Q_OUT_COUNT] += 1.0;
+    }
+    acc[XAC_ST_MAX_T] = fmax(acc[XAC_ST_MAX_T], (double)T);
+    acc[XAC_ST_SUM_T] += (double)T;
+    acc[XAC_ST_COUNT_T] += 1.0;
+  }
+  block_reduce<kNStats>(acc, spec, rows + (long long)blockIdx.x * kNStats);
+}
+
+// ---- scalar metrics (generate_dataset.py:57-179) ------------------------------------------------
+enum MetricSlot : int {
+  kM_QVOL = 0,       // sum ux over outlet-labelled cells of plane x = nx-1
+  kM_N_IN,           // non-solid cells of plane x = 1
+  kM_RHO_IN,         //   sum rho there
+  kM_N_OUT,          // non-solid cells of plane x = nx-2
+  kM_RHO_OUT,        //   sum rho there
+  kM_TS_MAX,         // floor z = 0, x in [buf, buf+core_nx), y < core_ny
+  kM_TS_SUM,
+  kM_TS_SQ,
+  kM_TS_MIN,
+  kM_TS_N,
+  kM_QOUT,           // sum ux*T over outlet-labelled cells of plane x = nx-1
+  kM_TF_SUM,         // T over non-solid cells of the core box [buf, nx-buf) x [1, ny-1) x [4, nz-2)
+  kM_TF_N,
+  kM_RHO1_ALL,       // sum rho over all cells of plane x = 1
+  kM_RHO2_ALL,       // sum rho over all cells of plane x = nx-2
+  kM_MAXV,           // max |u| over all cells
+  kM_MAXT,
+  kM_TSUM_ALL,
+  kM_VFLUID,         // non-solid cells of the core box (compute_hydraulic_diameter)
+  kM_FACES,          // solid/non-solid face pairs inside the core box
+  kM_CORE_SOLID,     // solid cells in x in [buf, nx-buf) (compute_porosity)
+  kNMetrics
+};
+
+inline ReduceSpec<kNMetrics> metric_spec() {
+  ReduceSpec<kNMetrics> s{};
+  for (int k = 0; k < kNMetrics; ++k) s.op[k] = kSum;
+  s.op[kM_TS_MAX] = kMax;
+  s.op[kM_TS_MIN] = kMin;
+  s.op[kM_MAXV] = kMax;
+  s.op[kM_MAXT] = kMax;
+  return s;
+}
+
+struct MetricBox {
+  int buf, core_nx, core_ny;
+};
+
+__global__ void __launch_bounds__(256) metric_partials_kernel(FieldView v, MetricBox b, ReduceSpec<kNMetrics> spec,
+                                                              double* __restrict__ rows) {
+  double acc[kNMetrics];
+#pragma unroll
+  for (int k = 0; k < kNMetrics; ++k) acc[k] = identity(spec.op[k]);
+  const long long n = (long long)v.nx * v.ny * v.nz;
+  const int nx = v.nx, ny = v.ny, nz = v.nz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx);
+    const long long t = i / nx;
+    const int y = (int)(t % ny), z = (int)(t / ny);
+    const long long cell = x * v.sx + y * v.sy + z * v.sz;
+    const int m = view_type(v, cell);
+    const bool solid = m == kSolid;
+    const float ux = v.ux[cell * v.ustride], uy = v.uy[cell * v.ustride], uz = v.uz[cell * v.ustride];
+    const float r = v.rho[cell], T = v.T[cell];
+    if (x == nx - 1 && m == kOutlet) {
+      acc[kM_QVOL] += (double)ux;
+      acc[kM_QOUT] += (double)ux * (double)T;
+    }
+    if (x == 1) {
+      acc[kM_RHO1_ALL] += (double)r;
+      if (!solid) {
+        acc[kM_N_IN] += 1.0;
+        acc[kM_RHO_IN] += (double)r;
+      }
+    }
+    if (x == nx - 2) {
+      acc[kM_RHO2_ALL] += (double)r;
+      if (!solid) {
+        acc[kM_N_OUT] += 1.0;
+        acc[kM_RHO_OUT] += (double)r;
+      }
+    }
+    if (z == 0 && x >= b.buf && x < b.buf + b.core_nx && y < b.core_ny) {
+      acc[kM_TS_MAX] = fmax(acc[kM_TS_MAX], (double)T);
+      acc[kM_TS_MIN] = fmin(acc[kM_TS_MIN], (double)T);
+      acc[kM_TS_SUM] += (double)T;
+      acc[kM_TS_SQ] += (double)T * (double)T;
+      acc[kM_TS_N] += 1.0;
+    }
+    const bool in_core = x >= b.buf && x < nx - b.buf && y >= 1 && y < ny - 1 && z >= 4 && z < nz - 2;
+    if (in_core) {
+      if (!solid) {
+        acc[kM_TF_SUM] += (double)T;
+        acc[kM_TF_N] += 1.0;
+        acc[kM_VFLUID] += 1.0;
+      }
+      // faces to the +x, +y, +z neighbour when it is inside the core box too
+      if (x + 1 < nx - b.buf && (view_type(v, cell + v.sx) == kSolid) != solid) acc[kM_FACES] += 1.0;
+      if (y + 1 < ny - 1 && (view_type(v, cell + v.sy) == kSolid) != solid) acc[kM_FACES] += 1.0;
+      if (z + 1 < nz - 2 && (view_type(v, cell + v.sz) == kSolid) != solid) acc[kM_FACES] += 1.0;
+    }
+    if (x >= b.buf && x < nx - b.buf && solid) acc[kM_CORE_SOLID] += 1.0;
+    const double vm = sqrt((double)ux * ux + (double)uy * uy + (double)uz * uz);
+    acc[kM_MAXV] = fmax(acc[kM_MAXV], vm);
+    acc[kM_MAXT] = fmax(acc[kM_MAXT], (double)T);
+    acc[kM_TSUM_ALL] += (double)T;
+  }
+  block_reduce<kNMetrics>(acc, spec, rows + (long long)blockIdx.x * kNMetrics);
+}
+
+}  // namespace xac
