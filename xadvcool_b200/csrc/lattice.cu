@@ -55,6 +55,13 @@ __global__ void build_link_kernel(const uint8_t* __restrict__ type, const float*
   }
   w |= (uint32_t)(type[c] & 3) << kTypeShift;
   if (qsrc[c] > 0.0f) w |= kHeatedBit;
+  if (x == 0) w |= kXLoBit;
+  if (x == g.nx - 1) w |= kXHiBit;
+  if (y == 0) w |= kYLoBit;
+  if (y == g.ny - 1) w |= kYHiBit;
+  if (z == 0) w |= kZLoBit;
+  if (z == g.nz - 1) w |= kZHiBit;
+  if (w & (kYLoBit | kYHiBit | kZLoBit | kZHiBit)) w |= kYZBit;
   link[c] = w;
 }
 
@@ -191,6 +198,12 @@ struct LatticeImpl {
     p.T_in = (float)t_inlet;
     p.rho_out = (float)rho_outlet;
     p.T_ref = precision == XAC_FP32 ? 0.0f : (float)t_inlet;
+    const long long nxy = (long long)g.nx * g.ny;
+    for (int i = 0; i < kQ; ++i) {
+      const long long off = ex_of(i) + (long long)ey_of(i) * g.nx + (long long)ez_of(i) * nxy;
+      p.plane[i] = (uint32_t)((long long)i * g.N);
+      p.pull[i] = (uint32_t)((long long)i * g.N - off);
+    }
     return p;
   }
 
@@ -336,7 +349,7 @@ struct LatticeImpl {
 int run_stats(const FieldView& v, double* rows, int nblocks, double* dev_out, double* host_out, cudaStream_t s) {
   const auto spec = stats_spec();
   stats_partials_kernel<<<nblocks, kBlock, 0, s>>>(v, spec, rows);
-  combine_rows_kernel<kNStats><<<1, 32, 0, s>>>(rows, nblocks, spec, dev_out);
+  combine_rows_kernel<kNStats><<<1, 32 * kNStats, 0, s>>>(rows, nblocks, spec, dev_out);
   XAC_CUDA(cudaGetLastError());
   XAC_CUDA(cudaMemcpyAsync(host_out, dev_out, kNStats * sizeof(double), cudaMemcpyDeviceToHost, s));
   XAC_CUDA(cudaStreamSynchronize(s));
@@ -347,7 +360,7 @@ int run_metrics(const FieldView& v, MetricBox b, double* rows, int nblocks, doub
                 cudaStream_t s) {
   const auto spec = metric_spec();
   metric_partials_kernel<<<nblocks, kBlock, 0, s>>>(v, b, spec, rows);
-  combine_rows_kernel<kNMetrics><<<1, 32, 0, s>>>(rows, nblocks, spec, dev_out);
+  combine_rows_kernel<kNMetrics><<<1, 32 * kNMetrics, 0, s>>>(rows, nblocks, spec, dev_out);
   XAC_CUDA(cudaGetLastError());
   XAC_CUDA(cudaMemcpyAsync(host_raw, dev_out, kNMetrics * sizeof(double), cudaMemcpyDeviceToHost, s));
   XAC_CUDA(cudaStreamSynchronize(s));
@@ -455,7 +468,8 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
   XAC_REQUIRE(d, "xac_lattice_create: null descriptor");
   XAC_REQUIRE(d->nx >= 3 && d->ny >= 1 && d->nz >= 1, "xac_lattice_create: lattice %d x %d x %d too small", d->nx,
               d->ny, d->nz);
-  XAC_REQUIRE((long long)d->nx * d->ny * d->nz < (1LL << 31), "xac_lattice_create: lattice too large");
+  XAC_REQUIRE((long long)d->nx * d->ny * d->nz * kQ < (1LL << 31),
+              "xac_lattice_create: lattice too large (19 x cells must stay below 2^31)");
   XAC_REQUIRE(d->mask, "xac_lattice_create: null mask");
   XAC_REQUIRE(d->tau_fluid > 0.5, "xac_lattice_create: tau_fluid must exceed 0.5 (got %g)", d->tau_fluid);
   XAC_REQUIRE(d->Pr > 0, "xac_lattice_create: Pr must be positive");

@@ -22,9 +22,25 @@ namespace xac {
 // bits 0..18 : fluid pull of direction i bounces back (source out of the domain or solid)
 // bits 20..21: cell label (XAC_BC_*)
 // bit  22    : heated (heat_source * heat_power > 0)
+// bit  23/24 : x == 0 / x == nx-1
+// bits 26..29: y == 0, y == ny-1, z == 0, z == nz-1; bit 25 = any of them
+// With these bits a step needs no integer division to locate a cell.
 constexpr int kTypeShift = 20;
 constexpr uint32_t kHeatedBit = 1u << 22;
+constexpr uint32_t kXLoBit = 1u << 23;
+constexpr uint32_t kXHiBit = 1u << 24;
+constexpr uint32_t kYZBit = 1u << 25;
+constexpr uint32_t kYLoBit = 1u << 26;
+constexpr uint32_t kYHiBit = 1u << 27;
+constexpr uint32_t kZLoBit = 1u << 28;
+constexpr uint32_t kZHiBit = 1u << 29;
 __device__ __forceinline__ int link_type(uint32_t lw) { return (int)((lw >> kTypeShift) & 3u); }
+
+// wall bits that make the thermal source of direction I leave the domain through a y/z face
+__host__ __device__ constexpr uint32_t wall_bits(int I) {
+  return (ey_of(I) == 1 ? kYLoBit : 0u) | (ey_of(I) == -1 ? kYHiBit : 0u) | (ez_of(I) == 1 ? kZLoBit : 0u) |
+         (ez_of(I) == -1 ? kZHiBit : 0u);
+}
 
 struct Geom {
   int nx, ny, nz;
@@ -66,11 +82,24 @@ struct StepParams {
   float T_in;     // inlet temperature (thermal_engine3d.py:151)
   float rho_out;  // outlet density (simulation.py:61)
   float T_ref;    // thermal rest reference for 16-bit storage
+  // element offsets, modulo 2^32: plane[i] = i*N; pull[i] = i*N - (ex + ey*nx + ez*nx*ny), so that the
+  // source of direction i for cell c is pop[c + pull[i]] and its own value is pop[c + plane[i]]
+  uint32_t plane[kQ];
+  uint32_t pull[kQ];
 };
 
-// Equilibrium for all 19 directions with reference operand order, collision into out[].
 #define XAC_FOR19(M) M(0) M(1) M(2) M(3) M(4) M(5) M(6) M(7) M(8) M(9) M(10) M(11) M(12) M(13) M(14) M(15) M(16) M(17) M(18)
 
+// Lanes sharing one 32-byte DRAM sector of a population plane (planes are 256-byte aligned).
+template <typename S>
+__device__ __forceinline__ unsigned sector_group(int lane) {
+  return sizeof(S) == 4 ? (0xFFu << (lane & ~7)) : (0xFFFFu << (lane & ~15));
+}
+
+// One coupled step for one cell per thread (see the scheme at the top of this file). Solid cells carry no
+// fluid work: their fluid populations are the rest equilibrium w_i for ever (fluid_engine3d.py:193-194 never
+// streams them, and they start at rho=1, u=0); a solid lane still stores w_i when a fluid lane shares its
+// sector, so every sector of the fluid output is written whole.
 template <typename S, bool kMacro, bool kOwn>
 __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__ Pin, S* __restrict__ Pout,
                                                            const S* __restrict__ Qin, S* __restrict__ Qout,
@@ -80,33 +109,29 @@ __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__
                                                            float* __restrict__ rho_o, float* __restrict__ ux_o,
                                                            float* __restrict__ uy_o, float* __restrict__ uz_o,
                                                            const float* __restrict__ T0, StepParams p) {
-  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (c >= p.g.ncell) return;
-  const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz;
-  const long long nxy = (long long)nx * ny;
-  const long long N = p.g.N;
-  const int x = (int)(c % nx);
-  const long long t = c / nx;
-  const int y = (int)(t % ny);
-  const int z = (int)(t / ny);
-  const uint32_t lw = __ldg(link + c);
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = c < (uint32_t)p.g.ncell;
+  const uint32_t lw = valid ? __ldg(link + c) : ((uint32_t)kSolid << kTypeShift);
   const int type = link_type(lw);
+  const bool fluid = valid && type != kSolid;
+  const unsigned fluid_lanes = __ballot_sync(0xffffffffu, fluid);
+  const int lane = threadIdx.x & 31;
 
   float ux = 0.0f, uy = 0.0f, uz = 0.0f;
 
   // ------------------------------------------------------------------ fluid lattice
-  if (type != kSolid) {
+  if (fluid) {
     float F[kQ];
     if (type == kInlet) {
       // src/fluid_engine3d.py:197-244: no pull; unknown populations from the known ones
       float k[kQ];
-#define XAC_LD_OWN(I) k[I] = Pop<S>::ld(Pin + (long long)I * N + c, w_of(I));
+#define XAC_LD_OWN(I) k[I] = Pop<S>::ld(Pin + c + p.plane[I], w_of(I));
       XAC_FOR19(XAC_LD_OWN)
 #undef XAC_LD_OWN
       const float ux_in = __ldg(u_in_ptr);
       const float rn = (((((((((k[0] + k[3]) + k[4]) + k[5]) + k[6]) + k[15]) + k[16]) + k[17]) + k[18]) +
-                         2.0f * ((((k[2] + k[8]) + k[10]) + k[12]) + k[14])) /
-                        (1.0f - ux_in);
+                        2.0f * ((((k[2] + k[8]) + k[10]) + k[12]) + k[14])) /
+                       (1.0f - ux_in);
       const float c23 = 2.0f / 3.0f, c16 = 1.0f / 6.0f;
       F[0] = k[0];
       F[1] = k[2] + (c23 * rn) * ux_in;
@@ -129,10 +154,10 @@ __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__
       F[18] = k[18];
     } else if (type == kOutlet) {
       // src/fluid_engine3d.py:247-259: copy post-collision (x-1) and rescale to rho_outlet
-      const long long s = x > 0 ? c - 1 : c;
+      const uint32_t s = (lw & kXLoBit) ? c : c - 1;
       float sum = 0.0f;
-#define XAC_LD_OUT(I)                                     \
-  F[I] = Pop<S>::ld(Pin + (long long)I * N + s, w_of(I)); \
+#define XAC_LD_OUT(I)                                  \
+  F[I] = Pop<S>::ld(Pin + s + p.plane[I], w_of(I));    \
   sum += F[I];
       XAC_FOR19(XAC_LD_OUT)
 #undef XAC_LD_OUT
@@ -143,13 +168,8 @@ __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__
       }
     } else {
       // src/fluid_engine3d.py:262-272: pull, halfway bounce-back on out-of-domain or solid sources
-#define XAC_LD_PULL(I)                                                                                      \
-  {                                                                                                         \
-    constexpr int o = opp_of(I);                                                                            \
-    const long long off = (long long)ex_of(I) + (long long)ey_of(I) * nx + (long long)ez_of(I) * nxy;       \
-    const S* src = ((lw >> I) & 1u) ? (Pin + (long long)o * N + c) : (Pin + (long long)I * N + c - off);    \
-    F[I] = Pop<S>::ld(src, w_of(I));                                                                        \
-  }
+#define XAC_LD_PULL(I) \
+  F[I] = Pop<S>::ld(Pin + c + (((lw >> I) & 1u) ? p.plane[opp_of(I)] : p.pull[I]), w_of(I));
       XAC_FOR19(XAC_LD_PULL)
 #undef XAC_LD_PULL
     }
@@ -176,36 +196,43 @@ __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__
     // src/fluid_engine3d.py:157-173 BGK with the equilibrium in registers
     const float omega = 1.0f / p.tau_f;
     const float usq15 = 1.5f * ((ux * ux + uy * uy) + uz * uz);
-#define XAC_COLLIDE(I)                                                               \
-  {                                                                                  \
-    const float fe = feq_term(w_of(I) * r, edotu<I>(ux, uy, uz), usq15);            \
-    Pop<S>::st(Pout + (long long)I * N + c, F[I] - omega * (F[I] - fe), w_of(I));    \
+#define XAC_COLLIDE(I)                                                            \
+  {                                                                               \
+    const float fe = feq_term(w_of(I) * r, edotu<I>(ux, uy, uz), usq15);         \
+    Pop<S>::st(Pout + c + p.plane[I], F[I] - omega * (F[I] - fe), w_of(I));       \
   }
     XAC_FOR19(XAC_COLLIDE)
 #undef XAC_COLLIDE
-  } else if (kMacro) {
-    // solid populations are never streamed (fluid_engine3d.py:193-194): moments of the frozen values
-    float r = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f;
+  } else if (valid) {
+    if (kMacro) {
+      // moments of the frozen solid populations, as the reference's macroscopic kernel computes them
+      float r = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f;
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) {
-      const float v = Pop<S>::ld(Pin + (long long)i * N + c, w_of(i));
-      r += v;
-      if (ex_of(i) != 0) mx += ex_of(i) > 0 ? v : -v;
-      if (ey_of(i) != 0) my += ey_of(i) > 0 ? v : -v;
-      if (ez_of(i) != 0) mz += ez_of(i) > 0 ? v : -v;
+      for (int i = 0; i < kQ; ++i) {
+        const float v = Pop<S>::ld(Pin + c + p.plane[i], w_of(i));
+        r += v;
+        if (ex_of(i) != 0) mx += ex_of(i) > 0 ? v : -v;
+        if (ey_of(i) != 0) my += ey_of(i) > 0 ? v : -v;
+        if (ez_of(i) != 0) mz += ez_of(i) > 0 ? v : -v;
+      }
+      rho_o[c] = r;
+      ux_o[c] = r > 1e-10f ? mx / r : 0.0f;
+      uy_o[c] = r > 1e-10f ? my / r : 0.0f;
+      uz_o[c] = r > 1e-10f ? mz / r : 0.0f;
     }
-    rho_o[c] = r;
-    ux_o[c] = r > 1e-10f ? mx / r : 0.0f;
-    uy_o[c] = r > 1e-10f ? my / r : 0.0f;
-    uz_o[c] = r > 1e-10f ? mz / r : 0.0f;
+    if (fluid_lanes & sector_group<S>(lane)) {
+#pragma unroll
+      for (int i = 0; i < kQ; ++i) Pop<S>::st(Pout + c + p.plane[i], w_of(i), w_of(i));
+    }
   }
+  if (!valid) return;
 
   // ------------------------------------------------------------------ thermal lattice
   const float Tb = p.T_ref;
   float G[kQ];
   float T;
   if (kOwn) {
-#define XAC_LD_G0(I) G[I] = Pop<S>::ld(Qin + (long long)I * N + c, w_of(I) * Tb);
+#define XAC_LD_G0(I) G[I] = Pop<S>::ld(Qin + c + p.plane[I], w_of(I) * Tb);
     XAC_FOR19(XAC_LD_G0)
 #undef XAC_LD_G0
     T = __ldg(T0 + c);
@@ -216,29 +243,36 @@ __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__
       for (int i = 0; i < kQ; ++i) G[i] = w_of(i) * p.T_in;
     } else if (type == kOutlet) {
       // src/thermal_engine3d.py:170-177
-      const long long s = x > 0 ? c - 1 : c;
-#define XAC_LD_GOUT(I) G[I] = Pop<S>::ld(Qin + (long long)I * N + s, w_of(I) * Tb);
+      const uint32_t s = (lw & kXLoBit) ? c : c - 1;
+#define XAC_LD_GOUT(I) G[I] = Pop<S>::ld(Qin + s + p.plane[I], w_of(I) * Tb);
       XAC_FOR19(XAC_LD_GOUT)
 #undef XAC_LD_GOUT
-    } else {
-      // src/thermal_engine3d.py:180-211: pull; x<0 sources are the inlet equilibrium, x>=nx sources copy the
-      // own value, other out-of-domain sources bounce back (adiabatic walls)
-#define XAC_LD_GPULL(I)                                                                                        \
+    } else if (!(lw & kYZBit)) {
+      // src/thermal_engine3d.py:180-211, cells away from the y/z faces: plain pull, except x<0 sources (inlet
+      // equilibrium) and x>=nx sources (own value). Addresses stay in bounds: an x<0 source reads the own cell.
+#define XAC_LD_GFAST(I)                                                                                        \
   {                                                                                                            \
-    constexpr int a = ex_of(I), b = ey_of(I), d = ez_of(I);                                                    \
-    const bool xlo = (a == 1 && x == 0);                                                                       \
-    const bool xhi = (a == -1 && x == nx - 1);                                                                 \
-    const bool wall = (b == 1 && y == 0) || (b == -1 && y == ny - 1) || (d == 1 && z == 0) ||                 \
-                      (d == -1 && z == nz - 1);                                                                \
-    const long long off = (long long)a + (long long)b * nx + (long long)d * nxy;                               \
-    /* the address is always in bounds: x<0 sources read the own cell and the value is replaced */         \
-    const S* src = (xhi || xlo) ? (Qin + (long long)I * N + c)                                                 \
-                                : (wall ? (Qin + (long long)opp_of(I) * N + c) : (Qin + (long long)I * N + c - off)); \
-    const float v = Pop<S>::ld(src, w_of(I) * Tb);                                                             \
+    uint32_t off = p.pull[I];                                                                                  \
+    if (ex_of(I) == 1) off = (lw & kXLoBit) ? p.plane[I] : off;                                                \
+    if (ex_of(I) == -1) off = (lw & kXHiBit) ? p.plane[I] : off;                                               \
+    const float v = Pop<S>::ld(Qin + c + off, w_of(I) * Tb);                                                   \
+    G[I] = (ex_of(I) == 1 && (lw & kXLoBit)) ? w_of(I) * p.T_in : v;                                           \
+  }
+      XAC_FOR19(XAC_LD_GFAST)
+#undef XAC_LD_GFAST
+    } else {
+      // the same rule with adiabatic bounce-back at the y/z faces
+#define XAC_LD_GSLOW(I)                                                                                        \
+  {                                                                                                            \
+    const bool xlo = ex_of(I) == 1 && (lw & kXLoBit);                                                          \
+    const bool xhi = ex_of(I) == -1 && (lw & kXHiBit);                                                         \
+    const bool wall = (lw & wall_bits(I)) != 0u;                                                               \
+    const uint32_t off = (xlo || xhi) ? p.plane[I] : (wall ? p.plane[opp_of(I)] : p.pull[I]);                  \
+    const float v = Pop<S>::ld(Qin + c + off, w_of(I) * Tb);                                                   \
     G[I] = xlo ? w_of(I) * p.T_in : v;                                                                         \
   }
-      XAC_FOR19(XAC_LD_GPULL)
-#undef XAC_LD_GPULL
+      XAC_FOR19(XAC_LD_GSLOW)
+#undef XAC_LD_GSLOW
     }
     // src/thermal_engine3d.py:214-224
     T = 0.0f;
@@ -250,18 +284,13 @@ __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__
   const float omega_t = 1.0f / (solid ? p.tau_ts : p.tau_tf);
   const float srcf = 1.0f - 0.5f * omega_t;
   const float q = (lw & kHeatedBit) ? __ldg(qsrc + c) : 0.0f;
-  if (solid) {
-    ux = 0.0f;
-    uy = 0.0f;
-    uz = 0.0f;
-  }
   const float usq15t = 1.5f * ((ux * ux + uy * uy) + uz * uz);
 #define XAC_TCOLLIDE(I)                                                          \
   {                                                                              \
     const float ge = feq_term(w_of(I) * T, edotu<I>(ux, uy, uz), usq15t);       \
     float v = G[I] - omega_t * (G[I] - ge);                                      \
     if (q > 0.0f) v += (w_of(I) * srcf) * q;                                     \
-    Pop<S>::st(Qout + (long long)I * N + c, v, w_of(I) * Tb);                    \
+    Pop<S>::st(Qout + c + p.plane[I], v, w_of(I) * Tb);                          \
   }
   XAC_FOR19(XAC_TCOLLIDE)
 #undef XAC_TCOLLIDE
@@ -272,37 +301,27 @@ template <typename S>
 __global__ void __launch_bounds__(256) thermal_finalize_kernel(const S* __restrict__ Qin,
                                                                const uint32_t* __restrict__ link,
                                                                float* __restrict__ T_o, StepParams p) {
-  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (c >= p.g.ncell) return;
-  const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz;
-  const long long nxy = (long long)nx * ny;
-  const long long N = p.g.N;
-  const int x = (int)(c % nx);
-  const long long t = c / nx;
-  const int y = (int)(t % ny);
-  const int z = (int)(t / ny);
-  const int type = link_type(__ldg(link + c));
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= (uint32_t)p.g.ncell) return;
+  const uint32_t lw = __ldg(link + c);
+  const int type = link_type(lw);
   const float Tb = p.T_ref;
   float T = 0.0f;
   if (type == kInlet) {
 #pragma unroll
     for (int i = 0; i < kQ; ++i) T += w_of(i) * p.T_in;
   } else if (type == kOutlet) {
-    const long long s = x > 0 ? c - 1 : c;
+    const uint32_t s = (lw & kXLoBit) ? c : c - 1;
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) T += Pop<S>::ld(Qin + (long long)i * N + s, w_of(i) * Tb);
+    for (int i = 0; i < kQ; ++i) T += Pop<S>::ld(Qin + s + p.plane[i], w_of(i) * Tb);
   } else {
 #define XAC_T_PULL(I)                                                                                          \
   {                                                                                                            \
-    constexpr int a = ex_of(I), b = ey_of(I), d = ez_of(I);                                                    \
-    const bool xlo = (a == 1 && x == 0);                                                                       \
-    const bool xhi = (a == -1 && x == nx - 1);                                                                 \
-    const bool wall = (b == 1 && y == 0) || (b == -1 && y == ny - 1) || (d == 1 && z == 0) ||                 \
-                      (d == -1 && z == nz - 1);                                                                \
-    const long long off = (long long)a + (long long)b * nx + (long long)d * nxy;                               \
-    const S* src = (xhi || xlo) ? (Qin + (long long)I * N + c)                                                 \
-                                : (wall ? (Qin + (long long)opp_of(I) * N + c) : (Qin + (long long)I * N + c - off)); \
-    const float v = Pop<S>::ld(src, w_of(I) * Tb);                                                             \
+    const bool xlo = ex_of(I) == 1 && (lw & kXLoBit);                                                          \
+    const bool xhi = ex_of(I) == -1 && (lw & kXHiBit);                                                         \
+    const bool wall = (lw & wall_bits(I)) != 0u;                                                               \
+    const uint32_t off = (xlo || xhi) ? p.plane[I] : (wall ? p.plane[opp_of(I)] : p.pull[I]);                  \
+    const float v = Pop<S>::ld(Qin + c + off, w_of(I) * Tb);                                                   \
     T += xlo ? w_of(I) * p.T_in : v;                                                                           \
   }
     XAC_FOR19(XAC_T_PULL)

@@ -65,15 +65,19 @@ __device__ __forceinline__ void block_reduce(double (&acc)[K], const ReduceSpec<
   }
 }
 
-// Combine nrows rows of K partials in row order (deterministic); one block, thread k owns column k.
+// Combine nrows rows of K partials; one warp per column, lanes stride the rows and a fixed shuffle tree
+// finishes, so the result does not depend on scheduling (launch with 32*K threads).
 template <int K>
 __global__ void combine_rows_kernel(const double* __restrict__ rows, int nrows, ReduceSpec<K> spec,
                                     double* __restrict__ out) {
-  const int k = threadIdx.x;
+  const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (k >= K) return;
-  double v = identity(spec.op[k]);
-  for (int r = 0; r < nrows; ++r) v = combine(spec.op[k], v, rows[(long long)r * K + k]);
-  out[k] = v;
+  const int op = spec.op[k];
+  double v = identity(op);
+  for (int r = lane; r < nrows; r += 32) v = combine(op, v, rows[(long long)r * K + k]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = combine(op, v, __shfl_down_sync(0xffffffffu, v, o));
+  if (lane == 0) out[k] = v;
 }
 
 // ---- convergence / divergence stats (XAC_ST_* order) --------------------------------------------
