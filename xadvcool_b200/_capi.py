@@ -97,6 +97,8 @@ SIGNATURES = {
     "xac_lattice_set_inlet": [_vp, _d, _vp],
     "xac_lattice_get_inlet": [_vp, C.POINTER(_d), _vp],
     "xac_lattice_steps_done": [_vp, C.POINTER(C.c_longlong)],
+    "xac_lattice_tune": [_vp, _i, _i],
+    "xac_lattice_get_tune": [_vp, C.POINTER(_i), C.POINTER(_i)],
     "xac_lattice_scalars": [_vp, C.POINTER(ScalarParams), _vp, _vp],
     "xac_scalars_fields": [_vp, _vp, _vp, _vp, _i, _i, _i, C.POINTER(ScalarParams), _vp, _vp],
     "xac_lattice_state_bytes": [_vp, C.POINTER(C.c_size_t)],

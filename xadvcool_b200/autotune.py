@@ -1,0 +1,95 @@
+"""Autotuner for the launch shape of the fused coupled step (threads per block x cells per thread).
+
+The shape changes only the schedule, never a result (every cell runs the same arithmetic). Candidates are
+timed with CUDA events on a scratch lattice built from the same inputs, so the caller's lattice does not
+advance. The winner is cached per (device, lattice shape, precision, solid fraction) in a JSON file
+(``$XAC_AUTOTUNE_CACHE``, default ``~/.cache/xadvcool_b200/autotune.json``).
+"""
+from __future__ import annotations
+
+import json
+import os
+from pathlib import Path
+
+import numpy as np
+import torch
+
+BLOCKS = (64, 128, 256)
+CELLS = (1, 2, 4)
+
+
+def _cache_path() -> Path:
+    return Path(os.environ.get("XAC_AUTOTUNE_CACHE", Path.home() / ".cache" / "xadvcool_b200" / "autotune.json"))
+
+
+def _key(device, shape, precision, solid_frac) -> str:
+    name = torch.cuda.get_device_name(device).replace(" ", "_")
+    return f"{name}|{shape[0]}x{shape[1]}x{shape[2]}|{precision}|solid{round(solid_frac, 1):.1f}"
+
+
+def _load_cache() -> dict:
+    p = _cache_path()
+    try:
+        return json.loads(p.read_text())
+    except Exception:
+        return {}
+
+
+def _store_cache(c: dict) -> None:
+    p = _cache_path()
+    try:
+        p.parent.mkdir(parents=True, exist_ok=True)
+        tmp = p.with_suffix(".tmp")
+        tmp.write_text(json.dumps(c, indent=1, sort_keys=True))
+        tmp.replace(p)
+    except OSError:
+        pass
+
+
+def time_config(lat, block: int, cells: int, steps: int = 100, repeats: int = 3) -> float:
+    """Mean microseconds per coupled step of ``lat`` with the given launch shape (advances ``lat``)."""
+    lat.tune(block, cells)
+    lat.step(steps)  # warm-up and graph instantiation
+    stream = torch.cuda.current_stream(lat.device)
+    best = float("inf")
+    for _ in range(repeats):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        lat.step(steps)
+        b.record(stream)
+        b.synchronize()
+        best = min(best, a.elapsed_time(b) * 1e3 / steps)
+    return best
+
+
+def autotune(mask, *, heat_source=None, precision="fp32", device="cuda", steps=100, use_cache=True,
+             lattice_kwargs=None) -> dict:
+    """Pick the fastest (block, cells_per_thread) for this design; returns {"block", "cells", "table"}."""
+    from .lattice import Lattice
+    mask = np.asarray(mask)
+    dev = torch.device(device)
+    key = _key(dev, mask.shape, precision, float((mask == 1).mean()))
+    cache = _load_cache() if use_cache else {}
+    if key in cache:
+        return cache[key]
+    kw = dict(lattice_kwargs or {})
+    table = {}
+    with Lattice(mask, heat_source=heat_source, precision=precision, device=dev, **kw) as scratch:
+        scratch.step(2)
+        for b in BLOCKS:
+            for c in CELLS:
+                table[f"{b}x{c}"] = round(time_config(scratch, b, c, steps=steps), 3)
+    best = min(table, key=table.get)
+    b, c = (int(v) for v in best.split("x"))
+    res = {"block": b, "cells": c, "us_per_step": table[best], "table": table}
+    if use_cache:
+        cache[key] = res
+        _store_cache(cache)
+    return res
+
+
+def apply(lat, mask=None, **kw) -> dict:
+    """Autotune for ``lat``'s design and set the winning shape on it."""
+    res = autotune(lat.mask if mask is None else mask, precision=lat.params["precision"], device=lat.device, **kw)
+    lat.tune(res["block"], res["cells"])
+    return res

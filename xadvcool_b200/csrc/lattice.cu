@@ -167,7 +167,10 @@ struct LatticeImpl {
   double tau_fluid = 0.6, Pr = 7.0, k_ratio = 628.0, u_inlet_nominal = 0.03, rho_outlet = 1.0, t_inlet = 25.0,
          heat_power = 0.1;
   float tau_th_f = 0.5f, tau_th_s = 0.5f;
+  float relax[5] = {1.0f, 1.0f, 1.0f, 0.5f, 0.5f};  // omega_f, omega_tf, omega_ts, srcf_f, srcf_s (device-computed)
   float u_in_host = 0.0f;
+  int tune_block = 256;  // threads per block of the step kernel
+  int tune_cells = 1;    // cells per thread
 
   void* P[2] = {nullptr, nullptr};
   void* Qb[2] = {nullptr, nullptr};
@@ -198,6 +201,11 @@ struct LatticeImpl {
     p.T_in = (float)t_inlet;
     p.rho_out = (float)rho_outlet;
     p.T_ref = precision == XAC_FP32 ? 0.0f : (float)t_inlet;
+    p.omega_f = relax[0];
+    p.omega_tf = relax[1];
+    p.omega_ts = relax[2];
+    p.srcf_f = relax[3];
+    p.srcf_s = relax[4];
     const long long nxy = (long long)g.nx * g.ny;
     for (int i = 0; i < kQ; ++i) {
       const long long off = ex_of(i) + (long long)ey_of(i) * g.nx + (long long)ez_of(i) * nxy;
@@ -225,26 +233,31 @@ struct LatticeImpl {
     if (capture) cudaStreamDestroy(capture);
   }
 
-  template <typename S>
-  int launch_step(cudaStream_t s, bool macro, bool own) {
-    const StepParams p = params();
+  template <typename S, int kCells>
+  void launch_cells(cudaStream_t s, bool macro, bool own, const StepParams& p) {
     const S* Pin = (const S*)P[cur];
     S* Pout = (S*)P[cur ^ 1];
     const S* Qin = (const S*)Qb[cur];
     S* Qout = (S*)Qb[cur ^ 1];
-    const unsigned grid = grid_for(g.ncell, kBlock);
-    if (macro && own)
-      coupled_step_kernel<S, true, true><<<grid, kBlock, 0, s>>>(Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux, uy,
-                                                                 uz, T, p);
-    else if (macro)
-      coupled_step_kernel<S, true, false><<<grid, kBlock, 0, s>>>(Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux, uy,
-                                                                  uz, T, p);
-    else if (own)
-      coupled_step_kernel<S, false, true><<<grid, kBlock, 0, s>>>(Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux,
-                                                                  uy, uz, T, p);
-    else
-      coupled_step_kernel<S, false, false><<<grid, kBlock, 0, s>>>(Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux,
-                                                                   uy, uz, T, p);
+    const int b = tune_block;
+    const unsigned grid = grid_for(g.ncell, b * kCells);
+#define XAC_LAUNCH(M, O) \
+  coupled_step_kernel<S, M, O, kCells><<<grid, b, 0, s>>>(Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux, uy, uz, T, p)
+    if (macro && own) XAC_LAUNCH(true, true);
+    else if (macro) XAC_LAUNCH(true, false);
+    else if (own) XAC_LAUNCH(false, true);
+    else XAC_LAUNCH(false, false);
+#undef XAC_LAUNCH
+  }
+
+  template <typename S>
+  int launch_step(cudaStream_t s, bool macro, bool own) {
+    const StepParams p = params();
+    switch (tune_cells) {
+      case 2: launch_cells<S, 2>(s, macro, own, p); break;
+      case 4: launch_cells<S, 4>(s, macro, own, p); break;
+      default: launch_cells<S, 1>(s, macro, own, p);
+    }
     cur ^= 1;
     return XAC_OK;
   }
@@ -535,6 +548,8 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
   XAC_CUDA(cudaMemcpyAsync(L.type, type.data(), n, cudaMemcpyHostToDevice, s));
   XAC_CUDA(cudaMemcpyAsync(L.qsrc, q.data(), n * sizeof(float), cudaMemcpyHostToDevice, s));
   set_scalar_kernel<<<1, 1, 0, s>>>(L.u_in, L.u_in_host);
+  relaxation_factors_kernel<<<1, 1, 0, s>>>((float)L.tau_fluid, L.tau_th_f, L.tau_th_s, (float*)L.red_out);
+  XAC_CUDA(cudaMemcpyAsync(L.relax, L.red_out, sizeof(L.relax), cudaMemcpyDeviceToHost, s));
   build_link_kernel<<<grid_for(n, kBlock), kBlock, 0, s>>>(L.type, L.qsrc, L.link, L.g);
   XAC_CUDA(cudaGetLastError());
   // host vectors go out of scope: make the copies complete first
@@ -655,6 +670,30 @@ int xac_lattice_set_inlet(xac_lattice* lat, double u_inlet, void* stream) {
 int xac_lattice_get_inlet(xac_lattice* lat, double* u_inlet, void*) {
   XAC_REQUIRE(lat && u_inlet, "xac_lattice_get_inlet: null pointer");
   *u_inlet = (double)lat->impl.u_in_host;
+  return XAC_OK;
+}
+
+int xac_lattice_tune(xac_lattice* lat, int block, int cells_per_thread) {
+  XAC_REQUIRE(lat, "xac_lattice_tune: null lattice");
+  XAC_REQUIRE(block == 64 || block == 128 || block == 256, "xac_lattice_tune: block must be 64, 128 or 256 (got %d)",
+              block);
+  XAC_REQUIRE(cells_per_thread == 1 || cells_per_thread == 2 || cells_per_thread == 4,
+              "xac_lattice_tune: cells_per_thread must be 1, 2 or 4 (got %d)", cells_per_thread);
+  LatticeImpl& L = lat->impl;
+  std::lock_guard<std::mutex> g(L.mu);
+  if (L.tune_block != block || L.tune_cells != cells_per_thread) {
+    for (auto& kv : L.graphs) cudaGraphExecDestroy(kv.second);
+    L.graphs.clear();
+  }
+  L.tune_block = block;
+  L.tune_cells = cells_per_thread;
+  return XAC_OK;
+}
+
+int xac_lattice_get_tune(const xac_lattice* lat, int* block, int* cells_per_thread) {
+  XAC_REQUIRE(lat && block && cells_per_thread, "xac_lattice_get_tune: null pointer");
+  *block = lat->impl.tune_block;
+  *cells_per_thread = lat->impl.tune_cells;
   return XAC_OK;
 }
 

@@ -82,6 +82,9 @@ struct StepParams {
   float T_in;     // inlet temperature (thermal_engine3d.py:151)
   float rho_out;  // outlet density (simulation.py:61)
   float T_ref;    // thermal rest reference for 16-bit storage
+  // 1/tau and 1 - omega/2 computed once on the device (the same IEEE float division as in the reference's
+  // kernels, hoisted out of the per-cell work): fluid omega, thermal omega fluid/solid, source factor fluid/solid
+  float omega_f, omega_tf, omega_ts, srcf_f, srcf_s;
   // element offsets, modulo 2^32: plane[i] = i*N; pull[i] = i*N - (ex + ey*nx + ez*nx*ny), so that the
   // source of direction i for cell c is pop[c + pull[i]] and its own value is pop[c + plane[i]]
   uint32_t plane[kQ];
@@ -101,15 +104,13 @@ __device__ __forceinline__ unsigned sector_group(int lane) {
 // streams them, and they start at rho=1, u=0); a solid lane still stores w_i when a fluid lane shares its
 // sector, so every sector of the fluid output is written whole.
 template <typename S, bool kMacro, bool kOwn>
-__global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__ Pin, S* __restrict__ Pout,
-                                                           const S* __restrict__ Qin, S* __restrict__ Qout,
-                                                           const uint32_t* __restrict__ link,
-                                                           const float* __restrict__ qsrc,
-                                                           const float* __restrict__ u_in_ptr,
-                                                           float* __restrict__ rho_o, float* __restrict__ ux_o,
-                                                           float* __restrict__ uy_o, float* __restrict__ uz_o,
-                                                           const float* __restrict__ T0, StepParams p) {
-  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restrict__ Pin, S* __restrict__ Pout,
+                                             const S* __restrict__ Qin, S* __restrict__ Qout,
+                                             const uint32_t* __restrict__ link, const float* __restrict__ qsrc,
+                                             const float* __restrict__ u_in_ptr, float* __restrict__ rho_o,
+                                             float* __restrict__ ux_o, float* __restrict__ uy_o,
+                                             float* __restrict__ uz_o, const float* __restrict__ T0,
+                                             const StepParams& p) {
   const bool valid = c < (uint32_t)p.g.ncell;
   const uint32_t lw = valid ? __ldg(link + c) : ((uint32_t)kSolid << kTypeShift);
   const int type = link_type(lw);
@@ -194,7 +195,7 @@ __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__
       uz_o[c] = uz;
     }
     // src/fluid_engine3d.py:157-173 BGK with the equilibrium in registers
-    const float omega = 1.0f / p.tau_f;
+    const float omega = p.omega_f;
     const float usq15 = 1.5f * ((ux * ux + uy * uy) + uz * uz);
 #define XAC_COLLIDE(I)                                                            \
   {                                                                               \
@@ -281,8 +282,8 @@ __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__
   }
   // src/thermal_engine3d.py:105-145: tau by phase, u = 0 in solids, source w_i (1 - omega/2) q
   const bool solid = type == kSolid;
-  const float omega_t = 1.0f / (solid ? p.tau_ts : p.tau_tf);
-  const float srcf = 1.0f - 0.5f * omega_t;
+  const float omega_t = solid ? p.omega_ts : p.omega_tf;
+  const float srcf = solid ? p.srcf_s : p.srcf_f;
   const float q = (lw & kHeatedBit) ? __ldg(qsrc + c) : 0.0f;
   const float usq15t = 1.5f * ((ux * ux + uy * uy) + uz * uz);
 #define XAC_TCOLLIDE(I)                                                          \
@@ -294,6 +295,33 @@ __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__
   }
   XAC_FOR19(XAC_TCOLLIDE)
 #undef XAC_TCOLLIDE
+}
+
+// kCells cells per thread, at a stride of one block, so each load instruction stays coalesced.
+template <typename S, bool kMacro, bool kOwn, int kCells>
+__global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__ Pin, S* __restrict__ Pout,
+                                                           const S* __restrict__ Qin, S* __restrict__ Qout,
+                                                           const uint32_t* __restrict__ link,
+                                                           const float* __restrict__ qsrc,
+                                                           const float* __restrict__ u_in_ptr,
+                                                           float* __restrict__ rho_o, float* __restrict__ ux_o,
+                                                           float* __restrict__ uy_o, float* __restrict__ uz_o,
+                                                           const float* __restrict__ T0, StepParams p) {
+  const uint32_t base = blockIdx.x * blockDim.x * kCells + threadIdx.x;
+#pragma unroll
+  for (int j = 0; j < kCells; ++j)
+    coupled_cell<S, kMacro, kOwn>(base + j * blockDim.x, Pin, Pout, Qin, Qout, link, qsrc, u_in_ptr, rho_o, ux_o,
+                                  uy_o, uz_o, T0, p);
+}
+
+// omega and source factors, computed with the device's IEEE division once per lattice
+__global__ void relaxation_factors_kernel(float tau_f, float tau_tf, float tau_ts, float* out) {
+  const float of = 1.0f / tau_f, otf = 1.0f / tau_tf, ots = 1.0f / tau_ts;
+  out[0] = of;
+  out[1] = otf;
+  out[2] = ots;
+  out[3] = 1.0f - 0.5f * otf;
+  out[4] = 1.0f - 0.5f * ots;
 }
 
 // T^k = sum of the streamed thermal populations, without storing them (stats / field export steps).

@@ -89,6 +89,15 @@ class Lattice:
         _capi.call("xac_lattice_steps_done", self._h, C.byref(v))
         return int(v.value)
 
+    def tune(self, block: int, cells_per_thread: int):
+        """Launch shape of the fused step (threads per block, cells per thread); results are unaffected."""
+        _capi.call("xac_lattice_tune", self._h, int(block), int(cells_per_thread))
+
+    def get_tune(self):
+        b, c = C.c_int(), C.c_int()
+        _capi.call("xac_lattice_get_tune", self._h, C.byref(b), C.byref(c))
+        return int(b.value), int(c.value)
+
     def set_inlet(self, u_in: float):
         with torch.cuda.device(self.device):
             _capi.call("xac_lattice_set_inlet", self._h, float(u_in), stream_ptr(self.device))
