@@ -15,7 +15,7 @@ import numpy as np
 import torch
 
 BLOCKS = (64, 128, 256)
-CELLS = (1, 2, 4)
+CELLS = (1, 4)
 
 
 def _cache_path() -> Path:

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "lattice_kernels.cuh"
+#include "lattice_quad.cuh"
 #include "reductions.cuh"
 
 namespace xac {
@@ -169,8 +170,9 @@ struct LatticeImpl {
   float tau_th_f = 0.5f, tau_th_s = 0.5f;
   float relax[5] = {1.0f, 1.0f, 1.0f, 0.5f, 0.5f};  // omega_f, omega_tf, omega_ts, srcf_f, srcf_s (device-computed)
   float u_in_host = 0.0f;
-  int tune_block = 256;  // threads per block of the step kernel
-  int tune_cells = 1;    // cells per thread
+  int tune_block = 128;  // threads per block of the step kernel
+  int tune_cells = 1;    // cells per thread: 1 (per-cell kernel) or 4 (quad kernel)
+  bool quad_ok = false;  // nx % 4 == 0, inlets only at x = 0, outlets only at x = nx-1
 
   void* P[2] = {nullptr, nullptr};
   void* Qb[2] = {nullptr, nullptr};
@@ -233,30 +235,32 @@ struct LatticeImpl {
     if (capture) cudaStreamDestroy(capture);
   }
 
-  template <typename S, int kCells>
-  void launch_cells(cudaStream_t s, bool macro, bool own, const StepParams& p) {
+  template <typename S>
+  int launch_step(cudaStream_t s, bool macro, bool own) {
+    const StepParams p = params();
     const S* Pin = (const S*)P[cur];
     S* Pout = (S*)P[cur ^ 1];
     const S* Qin = (const S*)Qb[cur];
     S* Qout = (S*)Qb[cur ^ 1];
     const int b = tune_block;
-    const unsigned grid = grid_for(g.ncell, b * kCells);
+    if (tune_cells == 4 && quad_ok) {
+      const unsigned grid = grid_for(g.ncell / 4, b);
 #define XAC_LAUNCH(M, O) \
-  coupled_step_kernel<S, M, O, kCells><<<grid, b, 0, s>>>(Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux, uy, uz, T, p)
-    if (macro && own) XAC_LAUNCH(true, true);
-    else if (macro) XAC_LAUNCH(true, false);
-    else if (own) XAC_LAUNCH(false, true);
-    else XAC_LAUNCH(false, false);
+  coupled_step_quad_kernel<S, M, O><<<grid, b, 0, s>>>(Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux, uy, uz, T, p)
+      if (macro && own) XAC_LAUNCH(true, true);
+      else if (macro) XAC_LAUNCH(true, false);
+      else if (own) XAC_LAUNCH(false, true);
+      else XAC_LAUNCH(false, false);
 #undef XAC_LAUNCH
-  }
-
-  template <typename S>
-  int launch_step(cudaStream_t s, bool macro, bool own) {
-    const StepParams p = params();
-    switch (tune_cells) {
-      case 2: launch_cells<S, 2>(s, macro, own, p); break;
-      case 4: launch_cells<S, 4>(s, macro, own, p); break;
-      default: launch_cells<S, 1>(s, macro, own, p);
+    } else {
+      const unsigned grid = grid_for(g.ncell, b);
+#define XAC_LAUNCH(M, O) \
+  coupled_step_kernel<S, M, O, 1><<<grid, b, 0, s>>>(Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux, uy, uz, T, p)
+      if (macro && own) XAC_LAUNCH(true, true);
+      else if (macro) XAC_LAUNCH(true, false);
+      else if (own) XAC_LAUNCH(false, true);
+      else XAC_LAUNCH(false, false);
+#undef XAC_LAUNCH
     }
     cur ^= 1;
     return XAC_OK;
@@ -521,6 +525,18 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
         type[((size_t)z * ny + y) * nx + x] = (uint8_t)m;
       }
   std::vector<float> q = host_qsrc(d);
+  bool quad_ok = (nx % 4) == 0;
+  for (int x = 0; x < nx && quad_ok; ++x)
+    for (int y = 0; y < ny && quad_ok; ++y)
+      for (int z = 0; z < nz; ++z) {
+        const int m = type[((size_t)z * ny + y) * nx + x];
+        if ((m == kInlet && x != 0) || (m == kOutlet && x != nx - 1)) {
+          quad_ok = false;
+          break;
+        }
+      }
+  L.quad_ok = quad_ok;
+  L.tune_cells = quad_ok ? 4 : 1;
 
   const size_t pop_bytes = (size_t)kQ * L.g.N * L.pop_elem;
   for (int b = 0; b < 2; ++b) {
@@ -677,8 +693,8 @@ int xac_lattice_tune(xac_lattice* lat, int block, int cells_per_thread) {
   XAC_REQUIRE(lat, "xac_lattice_tune: null lattice");
   XAC_REQUIRE(block == 64 || block == 128 || block == 256, "xac_lattice_tune: block must be 64, 128 or 256 (got %d)",
               block);
-  XAC_REQUIRE(cells_per_thread == 1 || cells_per_thread == 2 || cells_per_thread == 4,
-              "xac_lattice_tune: cells_per_thread must be 1, 2 or 4 (got %d)", cells_per_thread);
+  XAC_REQUIRE(cells_per_thread == 1 || cells_per_thread == 4,
+              "xac_lattice_tune: cells_per_thread must be 1 or 4 (got %d)", cells_per_thread);
   LatticeImpl& L = lat->impl;
   std::lock_guard<std::mutex> g(L.mu);
   if (L.tune_block != block || L.tune_cells != cells_per_thread) {
@@ -686,7 +702,7 @@ int xac_lattice_tune(xac_lattice* lat, int block, int cells_per_thread) {
     L.graphs.clear();
   }
   L.tune_block = block;
-  L.tune_cells = cells_per_thread;
+  L.tune_cells = (cells_per_thread == 4 && L.quad_ok) ? 4 : 1;
   return XAC_OK;
 }
 

@@ -110,13 +110,10 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
                                              const float* __restrict__ u_in_ptr, float* __restrict__ rho_o,
                                              float* __restrict__ ux_o, float* __restrict__ uy_o,
                                              float* __restrict__ uz_o, const float* __restrict__ T0,
-                                             const StepParams& p) {
-  const bool valid = c < (uint32_t)p.g.ncell;
-  const uint32_t lw = valid ? __ldg(link + c) : ((uint32_t)kSolid << kTypeShift);
+                                             const StepParams& p, const bool valid, const uint32_t lw,
+                                             const bool fill_solid) {
   const int type = link_type(lw);
   const bool fluid = valid && type != kSolid;
-  const unsigned fluid_lanes = __ballot_sync(0xffffffffu, fluid);
-  const int lane = threadIdx.x & 31;
 
   float ux = 0.0f, uy = 0.0f, uz = 0.0f;
 
@@ -221,7 +218,7 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
       uy_o[c] = r > 1e-10f ? my / r : 0.0f;
       uz_o[c] = r > 1e-10f ? mz / r : 0.0f;
     }
-    if (fluid_lanes & sector_group<S>(lane)) {
+    if (fill_solid) {
 #pragma unroll
       for (int i = 0; i < kQ; ++i) Pop<S>::st(Pout + c + p.plane[i], w_of(i), w_of(i));
     }
@@ -308,10 +305,16 @@ __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__
                                                            float* __restrict__ uy_o, float* __restrict__ uz_o,
                                                            const float* __restrict__ T0, StepParams p) {
   const uint32_t base = blockIdx.x * blockDim.x * kCells + threadIdx.x;
+  const int lane = threadIdx.x & 31;
 #pragma unroll
-  for (int j = 0; j < kCells; ++j)
-    coupled_cell<S, kMacro, kOwn>(base + j * blockDim.x, Pin, Pout, Qin, Qout, link, qsrc, u_in_ptr, rho_o, ux_o,
-                                  uy_o, uz_o, T0, p);
+  for (int j = 0; j < kCells; ++j) {
+    const uint32_t c = base + j * blockDim.x;
+    const bool valid = c < (uint32_t)p.g.ncell;
+    const uint32_t lw = valid ? __ldg(link + c) : ((uint32_t)kSolid << kTypeShift);
+    const unsigned fluid_lanes = __ballot_sync(0xffffffffu, valid && link_type(lw) != kSolid);
+    coupled_cell<S, kMacro, kOwn>(c, Pin, Pout, Qin, Qout, link, qsrc, u_in_ptr, rho_o, ux_o, uy_o, uz_o, T0, p,
+                                  valid, lw, (fluid_lanes & sector_group<S>(lane)) != 0u);
+  }
 }
 
 // omega and source factors, computed with the device's IEEE division once per lattice
