@@ -211,8 +211,8 @@ struct LatticeImpl {
     const long long nxy = (long long)g.nx * g.ny;
     for (int i = 0; i < kQ; ++i) {
       const long long off = ex_of(i) + (long long)ey_of(i) * g.nx + (long long)ez_of(i) * nxy;
-      p.plane[i] = (uint32_t)((long long)i * g.N);
-      p.pull[i] = (uint32_t)((long long)i * g.N - off);
+      p.plane[i] = (int32_t)((long long)i * g.N);
+      p.pull[i] = (int32_t)((long long)i * g.N - off);
     }
     return p;
   }

@@ -85,10 +85,11 @@ struct StepParams {
   // 1/tau and 1 - omega/2 computed once on the device (the same IEEE float division as in the reference's
   // kernels, hoisted out of the per-cell work): fluid omega, thermal omega fluid/solid, source factor fluid/solid
   float omega_f, omega_tf, omega_ts, srcf_f, srcf_s;
-  // element offsets, modulo 2^32: plane[i] = i*N; pull[i] = i*N - (ex + ey*nx + ez*nx*ny), so that the
-  // source of direction i for cell c is pop[c + pull[i]] and its own value is pop[c + plane[i]]
-  uint32_t plane[kQ];
-  uint32_t pull[kQ];
+  // element offsets: plane[i] = i*N; pull[i] = i*N - (ex + ey*nx + ez*nx*ny), so that the source of direction i
+  // for cell c is pop[c + pull[i]] and its own value is pop[c + plane[i]]. Kernels form one 64-bit pointer per
+  // cell and add these warp-uniform offsets, which the hardware folds into the load/store address.
+  int32_t plane[kQ];
+  int32_t pull[kQ];
 };
 
 #define XAC_FOR19(M) M(0) M(1) M(2) M(3) M(4) M(5) M(6) M(7) M(8) M(9) M(10) M(11) M(12) M(13) M(14) M(15) M(16) M(17) M(18)
@@ -114,6 +115,10 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
                                              const bool fill_solid) {
   const int type = link_type(lw);
   const bool fluid = valid && type != kSolid;
+  const S* __restrict__ Pc = Pin + c;  // this cell's element in plane 0
+  const S* __restrict__ Qc = Qin + c;
+  S* __restrict__ Po = Pout + c;
+  S* __restrict__ Qo = Qout + c;
 
   float ux = 0.0f, uy = 0.0f, uz = 0.0f;
 
@@ -123,7 +128,7 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
     if (type == kInlet) {
       // src/fluid_engine3d.py:197-244: no pull; unknown populations from the known ones
       float k[kQ];
-#define XAC_LD_OWN(I) k[I] = Pop<S>::ld(Pin + c + p.plane[I], w_of(I));
+#define XAC_LD_OWN(I) k[I] = Pop<S>::ld(Pc + p.plane[I], w_of(I));
       XAC_FOR19(XAC_LD_OWN)
 #undef XAC_LD_OWN
       const float ux_in = __ldg(u_in_ptr);
@@ -152,10 +157,10 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
       F[18] = k[18];
     } else if (type == kOutlet) {
       // src/fluid_engine3d.py:247-259: copy post-collision (x-1) and rescale to rho_outlet
-      const uint32_t s = (lw & kXLoBit) ? c : c - 1;
+      const S* __restrict__ Ps = (lw & kXLoBit) ? Pc : Pc - 1;
       float sum = 0.0f;
-#define XAC_LD_OUT(I)                                  \
-  F[I] = Pop<S>::ld(Pin + s + p.plane[I], w_of(I));    \
+#define XAC_LD_OUT(I)                              \
+  F[I] = Pop<S>::ld(Ps + p.plane[I], w_of(I));     \
   sum += F[I];
       XAC_FOR19(XAC_LD_OUT)
 #undef XAC_LD_OUT
@@ -166,8 +171,8 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
       }
     } else {
       // src/fluid_engine3d.py:262-272: pull, halfway bounce-back on out-of-domain or solid sources
-#define XAC_LD_PULL(I) \
-  F[I] = Pop<S>::ld(Pin + c + (((lw >> I) & 1u) ? p.plane[opp_of(I)] : p.pull[I]), w_of(I));
+#define XAC_LD_PULL(I)                                                                                      \
+  F[I] = ((lw >> I) & 1u) ? Pop<S>::ld(Pc + p.plane[opp_of(I)], w_of(I)) : Pop<S>::ld(Pc + p.pull[I], w_of(I));
       XAC_FOR19(XAC_LD_PULL)
 #undef XAC_LD_PULL
     }
@@ -197,7 +202,7 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
 #define XAC_COLLIDE(I)                                                            \
   {                                                                               \
     const float fe = feq_term(w_of(I) * r, edotu<I>(ux, uy, uz), usq15);         \
-    Pop<S>::st(Pout + c + p.plane[I], F[I] - omega * (F[I] - fe), w_of(I));       \
+    Pop<S>::st(Po + p.plane[I], F[I] - omega * (F[I] - fe), w_of(I));             \
   }
     XAC_FOR19(XAC_COLLIDE)
 #undef XAC_COLLIDE
@@ -207,7 +212,7 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
       float r = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f;
 #pragma unroll
       for (int i = 0; i < kQ; ++i) {
-        const float v = Pop<S>::ld(Pin + c + p.plane[i], w_of(i));
+        const float v = Pop<S>::ld(Pc + p.plane[i], w_of(i));
         r += v;
         if (ex_of(i) != 0) mx += ex_of(i) > 0 ? v : -v;
         if (ey_of(i) != 0) my += ey_of(i) > 0 ? v : -v;
@@ -220,7 +225,7 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
     }
     if (fill_solid) {
 #pragma unroll
-      for (int i = 0; i < kQ; ++i) Pop<S>::st(Pout + c + p.plane[i], w_of(i), w_of(i));
+      for (int i = 0; i < kQ; ++i) Pop<S>::st(Po + p.plane[i], w_of(i), w_of(i));
     }
   }
   if (!valid) return;
@@ -230,7 +235,7 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
   float G[kQ];
   float T;
   if (kOwn) {
-#define XAC_LD_G0(I) G[I] = Pop<S>::ld(Qin + c + p.plane[I], w_of(I) * Tb);
+#define XAC_LD_G0(I) G[I] = Pop<S>::ld(Qc + p.plane[I], w_of(I) * Tb);
     XAC_FOR19(XAC_LD_G0)
 #undef XAC_LD_G0
     T = __ldg(T0 + c);
@@ -241,8 +246,8 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
       for (int i = 0; i < kQ; ++i) G[i] = w_of(i) * p.T_in;
     } else if (type == kOutlet) {
       // src/thermal_engine3d.py:170-177
-      const uint32_t s = (lw & kXLoBit) ? c : c - 1;
-#define XAC_LD_GOUT(I) G[I] = Pop<S>::ld(Qin + s + p.plane[I], w_of(I) * Tb);
+      const S* __restrict__ Qs = (lw & kXLoBit) ? Qc : Qc - 1;
+#define XAC_LD_GOUT(I) G[I] = Pop<S>::ld(Qs + p.plane[I], w_of(I) * Tb);
       XAC_FOR19(XAC_LD_GOUT)
 #undef XAC_LD_GOUT
     } else if (!(lw & kYZBit)) {
@@ -250,11 +255,12 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
       // equilibrium) and x>=nx sources (own value). Addresses stay in bounds: an x<0 source reads the own cell.
 #define XAC_LD_GFAST(I)                                                                                        \
   {                                                                                                            \
-    uint32_t off = p.pull[I];                                                                                  \
-    if (ex_of(I) == 1) off = (lw & kXLoBit) ? p.plane[I] : off;                                                \
-    if (ex_of(I) == -1) off = (lw & kXHiBit) ? p.plane[I] : off;                                               \
-    const float v = Pop<S>::ld(Qin + c + off, w_of(I) * Tb);                                                   \
-    G[I] = (ex_of(I) == 1 && (lw & kXLoBit)) ? w_of(I) * p.T_in : v;                                           \
+    if (ex_of(I) == 1)                                                                                         \
+      G[I] = (lw & kXLoBit) ? w_of(I) * p.T_in : Pop<S>::ld(Qc + p.pull[I], w_of(I) * Tb);                     \
+    else if (ex_of(I) == -1)                                                                                   \
+      G[I] = (lw & kXHiBit) ? Pop<S>::ld(Qc + p.plane[I], w_of(I) * Tb) : Pop<S>::ld(Qc + p.pull[I], w_of(I) * Tb); \
+    else                                                                                                       \
+      G[I] = Pop<S>::ld(Qc + p.pull[I], w_of(I) * Tb);                                                         \
   }
       XAC_FOR19(XAC_LD_GFAST)
 #undef XAC_LD_GFAST
@@ -265,9 +271,14 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
     const bool xlo = ex_of(I) == 1 && (lw & kXLoBit);                                                          \
     const bool xhi = ex_of(I) == -1 && (lw & kXHiBit);                                                         \
     const bool wall = (lw & wall_bits(I)) != 0u;                                                               \
-    const uint32_t off = (xlo || xhi) ? p.plane[I] : (wall ? p.plane[opp_of(I)] : p.pull[I]);                  \
-    const float v = Pop<S>::ld(Qin + c + off, w_of(I) * Tb);                                                   \
-    G[I] = xlo ? w_of(I) * p.T_in : v;                                                                         \
+    if (xlo)                                                                                                   \
+      G[I] = w_of(I) * p.T_in;                                                                                 \
+    else if (xhi)                                                                                              \
+      G[I] = Pop<S>::ld(Qc + p.plane[I], w_of(I) * Tb);                                                        \
+    else if (wall)                                                                                             \
+      G[I] = Pop<S>::ld(Qc + p.plane[opp_of(I)], w_of(I) * Tb);                                                \
+    else                                                                                                       \
+      G[I] = Pop<S>::ld(Qc + p.pull[I], w_of(I) * Tb);                                                         \
   }
       XAC_FOR19(XAC_LD_GSLOW)
 #undef XAC_LD_GSLOW
@@ -288,7 +299,7 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
     const float ge = feq_term(w_of(I) * T, edotu<I>(ux, uy, uz), usq15t);       \
     float v = G[I] - omega_t * (G[I] - ge);                                      \
     if (q > 0.0f) v += (w_of(I) * srcf) * q;                                     \
-    Pop<S>::st(Qout + c + p.plane[I], v, w_of(I) * Tb);                          \
+    Pop<S>::st(Qo + p.plane[I], v, w_of(I) * Tb);                                \
   }
   XAC_FOR19(XAC_TCOLLIDE)
 #undef XAC_TCOLLIDE
@@ -337,23 +348,31 @@ __global__ void __launch_bounds__(256) thermal_finalize_kernel(const S* __restri
   const uint32_t lw = __ldg(link + c);
   const int type = link_type(lw);
   const float Tb = p.T_ref;
+  const S* __restrict__ Qc = Qin + c;
   float T = 0.0f;
   if (type == kInlet) {
 #pragma unroll
     for (int i = 0; i < kQ; ++i) T += w_of(i) * p.T_in;
   } else if (type == kOutlet) {
-    const uint32_t s = (lw & kXLoBit) ? c : c - 1;
+    const S* __restrict__ Qs = (lw & kXLoBit) ? Qc : Qc - 1;
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) T += Pop<S>::ld(Qin + s + p.plane[i], w_of(i) * Tb);
+    for (int i = 0; i < kQ; ++i) T += Pop<S>::ld(Qs + p.plane[i], w_of(i) * Tb);
   } else {
 #define XAC_T_PULL(I)                                                                                          \
   {                                                                                                            \
     const bool xlo = ex_of(I) == 1 && (lw & kXLoBit);                                                          \
     const bool xhi = ex_of(I) == -1 && (lw & kXHiBit);                                                         \
     const bool wall = (lw & wall_bits(I)) != 0u;                                                               \
-    const uint32_t off = (xlo || xhi) ? p.plane[I] : (wall ? p.plane[opp_of(I)] : p.pull[I]);                  \
-    const float v = Pop<S>::ld(Qin + c + off, w_of(I) * Tb);                                                   \
-    T += xlo ? w_of(I) * p.T_in : v;                                                                           \
+    float v;                                                                                                   \
+    if (xlo)                                                                                                   \
+      v = w_of(I) * p.T_in;                                                                                    \
+    else if (xhi)                                                                                              \
+      v = Pop<S>::ld(Qc + p.plane[I], w_of(I) * Tb);                                                           \
+    else if (wall)                                                                                             \
+      v = Pop<S>::ld(Qc + p.plane[opp_of(I)], w_of(I) * Tb);                                                   \
+    else                                                                                                       \
+      v = Pop<S>::ld(Qc + p.pull[I], w_of(I) * Tb);                                                            \
+    T += v;                                                                                                    \
   }
     XAC_FOR19(XAC_T_PULL)
 #undef XAC_T_PULL

@@ -77,7 +77,10 @@ __device__ __forceinline__ float solid_rho() {
 }
 
 template <typename S, bool kMacro, bool kOwn>
-__global__ void __launch_bounds__(128) coupled_step_quad_kernel(const S* __restrict__ Pin, S* __restrict__ Pout,
+#ifndef XAC_QUAD_MIN_BLOCKS
+#define XAC_QUAD_MIN_BLOCKS 2
+#endif
+__global__ void __launch_bounds__(256, XAC_QUAD_MIN_BLOCKS) coupled_step_quad_kernel(const S* __restrict__ Pin, S* __restrict__ Pout,
                                                                 const S* __restrict__ Qin, S* __restrict__ Qout,
                                                                 const uint32_t* __restrict__ link,
                                                                 const float* __restrict__ qsrc,
@@ -170,41 +173,34 @@ __global__ void __launch_bounds__(128) coupled_step_quad_kernel(const S* __restr
   }
     XAC_FOR19(XAC_Q_PULL)
 #undef XAC_Q_PULL
-    if ((xlo && inlet0) || (xhi && outlet3)) {
-      // boundary quads: the inlet cell (x = 0) uses its own populations, the outlet cell (x = nx-1) those of x-1
-      float own[kQ][4];
-#define XAC_Q_OWN(I) QuadIO<S>::ld(own[I], Pin + c0 + p.plane[I], w_of(I));
-      XAC_FOR19(XAC_Q_OWN)
-#undef XAC_Q_OWN
-      if (xlo && inlet0) {
-        // src/fluid_engine3d.py:197-244
-        const float ux_in = __ldg(u_in_ptr);
-        const float rn = (((((((((own[0][0] + own[3][0]) + own[4][0]) + own[5][0]) + own[6][0]) + own[15][0]) +
-                              own[16][0]) + own[17][0]) + own[18][0]) +
-                          2.0f * ((((own[2][0] + own[8][0]) + own[10][0]) + own[12][0]) + own[14][0])) /
-                         (1.0f - ux_in);
-        const float c23 = 2.0f / 3.0f, c16 = 1.0f / 6.0f;
+    if (xlo && inlet0) {
+      // src/fluid_engine3d.py:197-244: the inlet cell (x = 0, cell 0) uses its own populations
 #pragma unroll
-        for (int i = 0; i < kQ; ++i) F[i][0] = own[i][0];
-        F[1][0] = own[2][0] + (c23 * rn) * ux_in;
-        F[7][0] = own[10][0] + (c16 * rn) * ux_in;
-        F[9][0] = own[8][0] + (c16 * rn) * ux_in;
-        F[11][0] = own[14][0] + (c16 * rn) * ux_in;
-        F[13][0] = own[12][0] + (c16 * rn) * ux_in;
+      for (int i = 0; i < kQ; ++i) F[i][0] = Pop<S>::ld(Pin + c0 + p.plane[i], w_of(i));
+      const float ux_in = __ldg(u_in_ptr);
+      const float rn = (((((((((F[0][0] + F[3][0]) + F[4][0]) + F[5][0]) + F[6][0]) + F[15][0]) + F[16][0]) +
+                          F[17][0]) + F[18][0]) +
+                        2.0f * ((((F[2][0] + F[8][0]) + F[10][0]) + F[12][0]) + F[14][0])) /
+                       (1.0f - ux_in);
+      const float c23 = 2.0f / 3.0f, c16 = 1.0f / 6.0f;
+      F[1][0] = F[2][0] + (c23 * rn) * ux_in;
+      F[7][0] = F[10][0] + (c16 * rn) * ux_in;
+      F[9][0] = F[8][0] + (c16 * rn) * ux_in;
+      F[11][0] = F[14][0] + (c16 * rn) * ux_in;
+      F[13][0] = F[12][0] + (c16 * rn) * ux_in;
+    }
+    if (xhi && outlet3) {
+      // src/fluid_engine3d.py:247-259: the outlet cell (x = nx-1, cell 3) copies x-1 and rescales
+      float sum = 0.0f;
+#pragma unroll
+      for (int i = 0; i < kQ; ++i) {
+        F[i][3] = Pop<S>::ld(Pin + c0 + 2 + p.plane[i], w_of(i));
+        sum += F[i][3];
       }
-      if (xhi && outlet3) {
-        // src/fluid_engine3d.py:247-259
-        float sum = 0.0f;
+      if (sum > 1e-6f) {
+        const float sc = p.rho_out / sum;
 #pragma unroll
-        for (int i = 0; i < kQ; ++i) {
-          F[i][3] = own[i][2];
-          sum += F[i][3];
-        }
-        if (sum > 1e-6f) {
-          const float sc = p.rho_out / sum;
-#pragma unroll
-          for (int i = 0; i < kQ; ++i) F[i][3] *= sc;
-        }
+        for (int i = 0; i < kQ; ++i) F[i][3] *= sc;
       }
     }
     // moments (src/fluid_engine3d.py:85-113) and BGK (src/fluid_engine3d.py:157-173), cell by cell
@@ -263,6 +259,9 @@ __global__ void __launch_bounds__(128) coupled_step_quad_kernel(const S* __restr
       }
     }
   }
+
+  // keep the thermal loads behind the fluid stores: the two 76-value working sets are never live together
+  asm volatile("" ::: "memory");
 
   // ------------------------------------------------------------------ thermal lattice
   const float Tb = p.T_ref;
