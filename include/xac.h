@@ -193,12 +193,12 @@ int xac_lattice_fields(xac_lattice *lat, float *rho, float *u, float *T, void *s
 int xac_lattice_set_inlet(xac_lattice *lat, double u_inlet, void *stream);
 int xac_lattice_get_inlet(xac_lattice *lat, double *u_inlet, void *stream);
 int xac_lattice_steps_done(const xac_lattice *lat, long long *steps);
-/* Launch shape of the fused step kernel: threads per block (64, 128, 256) and cells per thread: 1 (one cell
- * per thread) or 4 (a quad of x-consecutive cells per thread with 128-bit population access; used when
- * nx % 4 == 0 and inlets/outlets lie on the x = 0 / x = nx-1 planes, else 1). Results do not depend on it:
- * every cell runs the same arithmetic. xadvcool_b200.autotune picks it. */
-int xac_lattice_tune(xac_lattice *lat, int block, int cells_per_thread);
-int xac_lattice_get_tune(const xac_lattice *lat, int *block, int *cells_per_thread);
+/* Launch shape of the fused step kernel: threads per block (64, 128, 256) and the visiting order:
+ * variant 0 = one thread per cell in memory order; variant 1 = cells grouped by class (bulk fluid, bulk solid,
+ * inlet/outlet/y-z-face cells) so that a warp never mixes the fluid and thermal-only work. Results do not depend
+ * on it (every cell runs the same arithmetic); xadvcool_b200.autotune picks it. */
+int xac_lattice_tune(xac_lattice *lat, int block, int variant);
+int xac_lattice_get_tune(const xac_lattice *lat, int *block, int *variant);
 /* Inputs of generate_dataset.py:80 compute_macroscopic_metrics that are not fields. */
 typedef struct xac_scalar_params {
     int buf;            /* inlet/outlet buffer length along x (10, generate_dataset.py:90)            */

@@ -201,27 +201,27 @@ def test_16bit_storage_error_vs_fp64_oracle(precision, tol_u, tol_T, cuda):
 @pytest.mark.parametrize("precision", ["fp32", "fp16", "bf16"])
 @pytest.mark.parametrize("block", [64, 128, 256])
 def test_launch_shapes_give_identical_bits(precision, block, cuda):
-    """Per-cell kernel and quad kernel (4 x-consecutive cells per thread) at every block size: same bits."""
+    """Memory-order and class-grouped visiting orders at every block size: same bits (and the oracle's)."""
     mask, hs, u_in, _ = designs.gyroid_design(3, nx=48, ny=20, nz=12)
     kw = dict(heat_source=hs, tau_fluid=0.56, u_inlet_val=u_in, heat_power=0.05, precision=precision)
     out = {}
-    for cells in (1, 4):
+    for variant in (0, 1):
         lat = Lattice(mask, **kw)
-        lat.tune(block, cells)
-        assert lat.get_tune() == (block, cells)
+        lat.tune(block, variant)
+        assert lat.get_tune() == (block, variant)
         lat.step(37)
-        out[cells] = [t.cpu().numpy() for t in lat.fields()] + [lat.stats()]
+        out[variant] = [t.cpu().numpy() for t in lat.fields()] + [lat.stats()]
         lat.close()
-    for a, b in zip(out[1], out[4]):
+    for a, b in zip(out[0], out[1]):
         assert np.array_equal(a, b)
     if precision == "fp32":
         ref = oracle_fields(mask, 37, hs=hs, tau_fluid=0.56, u_inlet_val=u_in, heat_power=0.05)
-        assert_exact(ref, *out[4][:3])
+        assert_exact(ref, *out[1][:3])
 
 
-def test_quad_path_falls_back_when_not_eligible(cuda):
-    rng = np.random.default_rng(7)
-    mask = rng.choice([0, 0, 1, 2, 3], size=(18, 7, 6)).astype(np.int32)  # nx % 4 != 0, inlets anywhere
-    lat = Lattice(mask, tau_fluid=0.6)
-    lat.tune(128, 4)
-    assert lat.get_tune() == (128, 1)
+def test_tune_rejects_bad_shapes(cuda):
+    lat = Lattice(designs.straight_fin_plate(), tau_fluid=0.6)
+    with pytest.raises(Exception):
+        lat.tune(96, 0)
+    with pytest.raises(Exception):
+        lat.tune(128, 2)

@@ -1,4 +1,4 @@
-"""Autotuner for the launch shape of the fused coupled step (threads per block x cells per thread).
+"""Autotuner for the launch shape of the fused coupled step (threads per block x visiting order).
 
 The shape changes only the schedule, never a result (every cell runs the same arithmetic). Candidates are
 timed with CUDA events on a scratch lattice built from the same inputs, so the caller's lattice does not
@@ -15,7 +15,7 @@ import numpy as np
 import torch
 
 BLOCKS = (64, 128, 256)
-CELLS = (1, 4)
+VARIANTS = (0, 1)  # 0: memory order, 1: grouped by cell class
 
 
 def _cache_path() -> Path:
@@ -46,9 +46,9 @@ def _store_cache(c: dict) -> None:
         pass
 
 
-def time_config(lat, block: int, cells: int, steps: int = 100, repeats: int = 3) -> float:
+def time_config(lat, block: int, variant: int, steps: int = 100, repeats: int = 3) -> float:
     """Mean microseconds per coupled step of ``lat`` with the given launch shape (advances ``lat``)."""
-    lat.tune(block, cells)
+    lat.tune(block, variant)
     lat.step(steps)  # warm-up and graph instantiation
     stream = torch.cuda.current_stream(lat.device)
     best = float("inf")
@@ -64,7 +64,7 @@ def time_config(lat, block: int, cells: int, steps: int = 100, repeats: int = 3)
 
 def autotune(mask, *, heat_source=None, precision="fp32", device="cuda", steps=100, use_cache=True,
              lattice_kwargs=None) -> dict:
-    """Pick the fastest (block, cells_per_thread) for this design; returns {"block", "cells", "table"}."""
+    """Pick the fastest (block, variant) for this design; returns {"block", "variant", "us_per_step", "table"}."""
     from .lattice import Lattice
     mask = np.asarray(mask)
     dev = torch.device(device)
@@ -77,11 +77,11 @@ def autotune(mask, *, heat_source=None, precision="fp32", device="cuda", steps=1
     with Lattice(mask, heat_source=heat_source, precision=precision, device=dev, **kw) as scratch:
         scratch.step(2)
         for b in BLOCKS:
-            for c in CELLS:
-                table[f"{b}x{c}"] = round(time_config(scratch, b, c, steps=steps), 3)
+            for v in VARIANTS:
+                table[f"{b}x{v}"] = round(time_config(scratch, b, v, steps=steps), 3)
     best = min(table, key=table.get)
-    b, c = (int(v) for v in best.split("x"))
-    res = {"block": b, "cells": c, "us_per_step": table[best], "table": table}
+    b, v = (int(t) for t in best.split("x"))
+    res = {"block": b, "variant": v, "us_per_step": table[best], "table": table}
     if use_cache:
         cache[key] = res
         _store_cache(cache)
@@ -91,5 +91,5 @@ def autotune(mask, *, heat_source=None, precision="fp32", device="cuda", steps=1
 def apply(lat, mask=None, **kw) -> dict:
     """Autotune for ``lat``'s design and set the winning shape on it."""
     res = autotune(lat.mask if mask is None else mask, precision=lat.params["precision"], device=lat.device, **kw)
-    lat.tune(res["block"], res["cells"])
+    lat.tune(res["block"], res["variant"])
     return res

@@ -9,7 +9,6 @@
 #include <vector>
 
 #include "lattice_kernels.cuh"
-#include "lattice_quad.cuh"
 #include "reductions.cuh"
 
 namespace xac {
@@ -39,8 +38,9 @@ __device__ __forceinline__ long long ref_index(int x, int y, int z, int ny, int 
   return ((long long)x * ny + y) * nz + z;
 }
 
+// sector = cells per 32-byte DRAM sector of a population plane (8 for FP32, 16 for 16-bit storage)
 __global__ void build_link_kernel(const uint8_t* __restrict__ type, const float* __restrict__ qsrc,
-                                  uint32_t* __restrict__ link, Geom g) {
+                                  uint32_t* __restrict__ link, Geom g, int sector) {
   const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (c >= g.ncell) return;
   const int x = (int)(c % g.nx);
@@ -63,6 +63,14 @@ __global__ void build_link_kernel(const uint8_t* __restrict__ type, const float*
   if (z == 0) w |= kZLoBit;
   if (z == g.nz - 1) w |= kZHiBit;
   if (w & (kYLoBit | kYHiBit | kZLoBit | kZHiBit)) w |= kYZBit;
+  if (type[c] == kSolid) {
+    const long long s0 = c - c % sector;
+    for (long long k = s0; k < s0 + sector && k < g.ncell; ++k)
+      if (type[k] != kSolid) {
+        w |= kFillBit;
+        break;
+      }
+  }
   link[c] = w;
 }
 
@@ -171,8 +179,9 @@ struct LatticeImpl {
   float relax[5] = {1.0f, 1.0f, 1.0f, 0.5f, 0.5f};  // omega_f, omega_tf, omega_ts, srcf_f, srcf_s (device-computed)
   float u_in_host = 0.0f;
   int tune_block = 128;  // threads per block of the step kernel
-  int tune_cells = 1;    // cells per thread: 1 (per-cell kernel) or 4 (quad kernel)
-  bool quad_ok = false;  // nx % 4 == 0, inlets only at x = 0, outlets only at x = nx-1
+  int tune_variant = 1;  // 0: cells in memory order; 1: cells grouped by class (bulk fluid / bulk solid / other)
+  uint32_t* cells = nullptr;                 // class-grouped cell list (kNoCell padding)
+  uint32_t cells_len = 0, end_fluid = 0, end_solid = 0;
 
   void* P[2] = {nullptr, nullptr};
   void* Qb[2] = {nullptr, nullptr};
@@ -222,6 +231,7 @@ struct LatticeImpl {
     for (void* b : {P[0], P[1], Qb[0], Qb[1]}) cudaFree(b);
     cudaFree(type);
     cudaFree(link);
+    cudaFree(cells);
     cudaFree(qsrc);
     cudaFree(u_in);
     cudaFree(rho);
@@ -243,10 +253,11 @@ struct LatticeImpl {
     const S* Qin = (const S*)Qb[cur];
     S* Qout = (S*)Qb[cur ^ 1];
     const int b = tune_block;
-    if (tune_cells == 4 && quad_ok) {
-      const unsigned grid = grid_for(g.ncell / 4, b);
-#define XAC_LAUNCH(M, O) \
-  coupled_step_quad_kernel<S, M, O><<<grid, b, 0, s>>>(Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux, uy, uz, T, p)
+    if (tune_variant == 1) {
+      const unsigned grid = cells_len / b;
+#define XAC_LAUNCH(M, O)                                                                                   \
+  coupled_step_grouped_kernel<S, M, O><<<grid, b, 0, s>>>(cells, end_fluid, end_solid, Pin, Pout, Qin, Qout, \
+                                                          link, qsrc, u_in, rho, ux, uy, uz, T, p)
       if (macro && own) XAC_LAUNCH(true, true);
       else if (macro) XAC_LAUNCH(true, false);
       else if (own) XAC_LAUNCH(false, true);
@@ -525,19 +536,29 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
         type[((size_t)z * ny + y) * nx + x] = (uint8_t)m;
       }
   std::vector<float> q = host_qsrc(d);
-  bool quad_ok = (nx % 4) == 0;
-  for (int x = 0; x < nx && quad_ok; ++x)
-    for (int y = 0; y < ny && quad_ok; ++y)
-      for (int z = 0; z < nz; ++z) {
-        const int m = type[((size_t)z * ny + y) * nx + x];
-        if ((m == kInlet && x != 0) || (m == kOutlet && x != nx - 1)) {
-          quad_ok = false;
-          break;
-        }
+  // class-grouped visiting order: bulk fluid, bulk solid, then inlet/outlet/y-z-face cells, each class in
+  // memory order and padded to a multiple of 512 entries
+  std::vector<uint32_t> lists[3];
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const uint32_t c = (uint32_t)(((size_t)z * ny + y) * nx + x);
+        const int m = type[c];
+        const bool face = y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
+        const int cls = face || m == kInlet || m == kOutlet ? kClassOther : (m == kSolid ? kClassBulkSolid
+                                                                                           : kClassBulkFluid);
+        lists[cls].push_back(c);
       }
-  L.quad_ok = quad_ok;
-  L.tune_cells = quad_ok ? 4 : 1;
-
+  std::vector<uint32_t> cells;
+  uint32_t ends[3];
+  for (int k = 0; k < 3; ++k) {
+    cells.insert(cells.end(), lists[k].begin(), lists[k].end());
+    while (cells.size() % 512) cells.push_back(kNoCell);
+    ends[k] = (uint32_t)cells.size();
+  }
+  L.cells_len = (uint32_t)cells.size();
+  L.end_fluid = ends[0];
+  L.end_solid = ends[1];
   const size_t pop_bytes = (size_t)kQ * L.g.N * L.pop_elem;
   for (int b = 0; b < 2; ++b) {
     XAC_CUDA(cudaMalloc(&L.P[b], pop_bytes));
@@ -546,6 +567,7 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
   int r;
   if ((r = dmalloc(&L.type, n, "alloc type")) != XAC_OK) return r;
   if ((r = dmalloc(&L.link, n, "alloc link")) != XAC_OK) return r;
+  if ((r = dmalloc(&L.cells, L.cells_len, "alloc cell list")) != XAC_OK) return r;
   if ((r = dmalloc(&L.qsrc, n, "alloc qsrc")) != XAC_OK) return r;
   if ((r = dmalloc(&L.u_in, 1, "alloc u_in")) != XAC_OK) return r;
   for (float** f : {&L.rho, &L.ux, &L.uy, &L.uz, &L.T})
@@ -562,11 +584,12 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
     XAC_CUDA(cudaMemsetAsync(L.Qb[b], 0, pop_bytes, s));
   }
   XAC_CUDA(cudaMemcpyAsync(L.type, type.data(), n, cudaMemcpyHostToDevice, s));
+  XAC_CUDA(cudaMemcpyAsync(L.cells, cells.data(), cells.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
   XAC_CUDA(cudaMemcpyAsync(L.qsrc, q.data(), n * sizeof(float), cudaMemcpyHostToDevice, s));
   set_scalar_kernel<<<1, 1, 0, s>>>(L.u_in, L.u_in_host);
   relaxation_factors_kernel<<<1, 1, 0, s>>>((float)L.tau_fluid, L.tau_th_f, L.tau_th_s, (float*)L.red_out);
   XAC_CUDA(cudaMemcpyAsync(L.relax, L.red_out, sizeof(L.relax), cudaMemcpyDeviceToHost, s));
-  build_link_kernel<<<grid_for(n, kBlock), kBlock, 0, s>>>(L.type, L.qsrc, L.link, L.g);
+  build_link_kernel<<<grid_for(n, kBlock), kBlock, 0, s>>>(L.type, L.qsrc, L.link, L.g, 32 / (int)L.pop_elem);
   XAC_CUDA(cudaGetLastError());
   // host vectors go out of scope: make the copies complete first
   XAC_CUDA(cudaStreamSynchronize(s));
@@ -689,27 +712,26 @@ int xac_lattice_get_inlet(xac_lattice* lat, double* u_inlet, void*) {
   return XAC_OK;
 }
 
-int xac_lattice_tune(xac_lattice* lat, int block, int cells_per_thread) {
+int xac_lattice_tune(xac_lattice* lat, int block, int variant) {
   XAC_REQUIRE(lat, "xac_lattice_tune: null lattice");
   XAC_REQUIRE(block == 64 || block == 128 || block == 256, "xac_lattice_tune: block must be 64, 128 or 256 (got %d)",
               block);
-  XAC_REQUIRE(cells_per_thread == 1 || cells_per_thread == 4,
-              "xac_lattice_tune: cells_per_thread must be 1 or 4 (got %d)", cells_per_thread);
+  XAC_REQUIRE(variant == 0 || variant == 1, "xac_lattice_tune: variant must be 0 or 1 (got %d)", variant);
   LatticeImpl& L = lat->impl;
   std::lock_guard<std::mutex> g(L.mu);
-  if (L.tune_block != block || L.tune_cells != cells_per_thread) {
+  if (L.tune_block != block || L.tune_variant != variant) {
     for (auto& kv : L.graphs) cudaGraphExecDestroy(kv.second);
     L.graphs.clear();
   }
   L.tune_block = block;
-  L.tune_cells = (cells_per_thread == 4 && L.quad_ok) ? 4 : 1;
+  L.tune_variant = variant;
   return XAC_OK;
 }
 
-int xac_lattice_get_tune(const xac_lattice* lat, int* block, int* cells_per_thread) {
-  XAC_REQUIRE(lat && block && cells_per_thread, "xac_lattice_get_tune: null pointer");
+int xac_lattice_get_tune(const xac_lattice* lat, int* block, int* variant) {
+  XAC_REQUIRE(lat && block && variant, "xac_lattice_get_tune: null pointer");
   *block = lat->impl.tune_block;
-  *cells_per_thread = lat->impl.tune_cells;
+  *variant = lat->impl.tune_variant;
   return XAC_OK;
 }
 

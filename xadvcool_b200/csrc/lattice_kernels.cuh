@@ -24,6 +24,8 @@ namespace xac {
 // bit  22    : heated (heat_source * heat_power > 0)
 // bit  23/24 : x == 0 / x == nx-1
 // bits 26..29: y == 0, y == ny-1, z == 0, z == nz-1; bit 25 = any of them
+// bit  30    : solid cell whose population sector also holds a non-solid cell (it stores w_i so that every
+//              fluid-output sector is written whole)
 // With these bits a step needs no integer division to locate a cell.
 constexpr int kTypeShift = 20;
 constexpr uint32_t kHeatedBit = 1u << 22;
@@ -34,6 +36,7 @@ constexpr uint32_t kYLoBit = 1u << 26;
 constexpr uint32_t kYHiBit = 1u << 27;
 constexpr uint32_t kZLoBit = 1u << 28;
 constexpr uint32_t kZHiBit = 1u << 29;
+constexpr uint32_t kFillBit = 1u << 30;  // solid cell sharing a 32-byte DRAM sector with a non-solid cell
 __device__ __forceinline__ int link_type(uint32_t lw) { return (int)((lw >> kTypeShift) & 3u); }
 
 // wall bits that make the thermal source of direction I leave the domain through a y/z face
@@ -325,6 +328,168 @@ __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__
     const unsigned fluid_lanes = __ballot_sync(0xffffffffu, valid && link_type(lw) != kSolid);
     coupled_cell<S, kMacro, kOwn>(c, Pin, Pout, Qin, Qout, link, qsrc, u_in_ptr, rho_o, ux_o, uy_o, uz_o, T0, p,
                                   valid, lw, (fluid_lanes & sector_group<S>(lane)) != 0u);
+  }
+}
+
+// ---- class-grouped step -------------------------------------------------------------------------
+// Cells are visited through an index list grouped by class, so a warp never mixes them:
+//   bulk fluid : fluid label, not on a y/z face  -> both lattices, plain pull, no boundary branches
+//   bulk solid : solid label, not on a y/z face  -> thermal lattice only, with u = 0, where the second-order
+//                equilibrium w_i T (1 + 3e.u + 4.5(e.u)^2 - 1.5u^2) evaluates to exactly w_i T
+//   other      : inlet, outlet and y/z-face cells -> the general per-cell path
+// Every cell runs exactly the arithmetic of coupled_cell, so results are identical.
+enum CellClass : int { kClassBulkFluid = 0, kClassBulkSolid = 1, kClassOther = 2 };
+constexpr uint32_t kNoCell = 0xFFFFFFFFu;
+
+template <typename S, bool kOwn>
+__device__ __forceinline__ void thermal_bulk_pull(const S* __restrict__ Qc, const uint32_t lw, const StepParams& p,
+                                                  const float* __restrict__ T0, const uint32_t c, float (&G)[kQ],
+                                                  float& T) {
+  const float Tb = p.T_ref;
+  if (kOwn) {
+#define XAC_LD_G0(I) G[I] = Pop<S>::ld(Qc + p.plane[I], w_of(I) * Tb);
+    XAC_FOR19(XAC_LD_G0)
+#undef XAC_LD_G0
+    T = __ldg(T0 + c);
+    return;
+  }
+#define XAC_LD_GFAST(I)                                                                                        \
+  {                                                                                                            \
+    if (ex_of(I) == 1)                                                                                         \
+      G[I] = (lw & kXLoBit) ? w_of(I) * p.T_in : Pop<S>::ld(Qc + p.pull[I], w_of(I) * Tb);                     \
+    else if (ex_of(I) == -1)                                                                                   \
+      G[I] = (lw & kXHiBit) ? Pop<S>::ld(Qc + p.plane[I], w_of(I) * Tb) : Pop<S>::ld(Qc + p.pull[I], w_of(I) * Tb); \
+    else                                                                                                       \
+      G[I] = Pop<S>::ld(Qc + p.pull[I], w_of(I) * Tb);                                                         \
+  }
+  XAC_FOR19(XAC_LD_GFAST)
+#undef XAC_LD_GFAST
+  T = 0.0f;
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) T += G[i];
+}
+
+template <typename S, bool kMacro, bool kOwn>
+__device__ __forceinline__ void bulk_fluid_cell(const uint32_t c, const uint32_t lw, const S* __restrict__ Pin,
+                                                S* __restrict__ Pout, const S* __restrict__ Qin,
+                                                S* __restrict__ Qout, const float* __restrict__ qsrc,
+                                                float* __restrict__ rho_o, float* __restrict__ ux_o,
+                                                float* __restrict__ uy_o, float* __restrict__ uz_o,
+                                                const float* __restrict__ T0, const StepParams& p) {
+  const S* __restrict__ Pc = Pin + c;
+  S* __restrict__ Po = Pout + c;
+  float F[kQ];
+#define XAC_LD_PULL(I)                                                                                      \
+  F[I] = ((lw >> I) & 1u) ? Pop<S>::ld(Pc + p.plane[opp_of(I)], w_of(I)) : Pop<S>::ld(Pc + p.pull[I], w_of(I));
+  XAC_FOR19(XAC_LD_PULL)
+#undef XAC_LD_PULL
+  float r = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f;
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    r += F[i];
+    if (ex_of(i) != 0) mx += ex_of(i) > 0 ? F[i] : -F[i];
+    if (ey_of(i) != 0) my += ey_of(i) > 0 ? F[i] : -F[i];
+    if (ez_of(i) != 0) mz += ez_of(i) > 0 ? F[i] : -F[i];
+  }
+  float ux = 0.0f, uy = 0.0f, uz = 0.0f;
+  if (r > 1e-10f) {
+    ux = mx / r;
+    uy = my / r;
+    uz = mz / r;
+  }
+  if (kMacro) {
+    rho_o[c] = r;
+    ux_o[c] = ux;
+    uy_o[c] = uy;
+    uz_o[c] = uz;
+  }
+  const float omega = p.omega_f;
+  const float usq15 = 1.5f * ((ux * ux + uy * uy) + uz * uz);
+#define XAC_COLLIDE(I)                                                            \
+  {                                                                               \
+    const float fe = feq_term(w_of(I) * r, edotu<I>(ux, uy, uz), usq15);         \
+    Pop<S>::st(Po + p.plane[I], F[I] - omega * (F[I] - fe), w_of(I));             \
+  }
+  XAC_FOR19(XAC_COLLIDE)
+#undef XAC_COLLIDE
+  float G[kQ], T;
+  thermal_bulk_pull<S, kOwn>(Qin + c, lw, p, T0, c, G, T);
+  S* __restrict__ Qo = Qout + c;
+  const float omega_t = p.omega_tf, srcf = p.srcf_f;
+  const float q = (lw & kHeatedBit) ? __ldg(qsrc + c) : 0.0f;
+  const float usq15t = 1.5f * ((ux * ux + uy * uy) + uz * uz);
+  const float Tb = p.T_ref;
+#define XAC_TCOLLIDE(I)                                                          \
+  {                                                                              \
+    const float ge = feq_term(w_of(I) * T, edotu<I>(ux, uy, uz), usq15t);       \
+    float v = G[I] - omega_t * (G[I] - ge);                                      \
+    if (q > 0.0f) v += (w_of(I) * srcf) * q;                                     \
+    Pop<S>::st(Qo + p.plane[I], v, w_of(I) * Tb);                                \
+  }
+  XAC_FOR19(XAC_TCOLLIDE)
+#undef XAC_TCOLLIDE
+}
+
+template <typename S, bool kMacro, bool kOwn>
+__device__ __forceinline__ void bulk_solid_cell(const uint32_t c, const uint32_t lw, S* __restrict__ Pout,
+                                                const S* __restrict__ Qin, S* __restrict__ Qout,
+                                                const float* __restrict__ qsrc, float* __restrict__ rho_o,
+                                                float* __restrict__ ux_o, float* __restrict__ uy_o,
+                                                float* __restrict__ uz_o, const float* __restrict__ T0,
+                                                const StepParams& p) {
+  if (kMacro) {
+    // the frozen solid populations are w_i: rho = sum of w_i in order, u = 0
+    float r = 0.0f;
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) r += w_of(i);
+    rho_o[c] = r;
+    ux_o[c] = 0.0f;
+    uy_o[c] = 0.0f;
+    uz_o[c] = 0.0f;
+  }
+  if (lw & kFillBit) {
+    S* __restrict__ Po = Pout + c;
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) Pop<S>::st(Po + p.plane[i], w_of(i), w_of(i));
+  }
+  float G[kQ], T;
+  thermal_bulk_pull<S, kOwn>(Qin + c, lw, p, T0, c, G, T);
+  S* __restrict__ Qo = Qout + c;
+  const float omega_t = p.omega_ts, srcf = p.srcf_s;
+  const float q = (lw & kHeatedBit) ? __ldg(qsrc + c) : 0.0f;
+  const float Tb = p.T_ref;
+#define XAC_TCOLLIDE_S(I)                                                        \
+  {                                                                              \
+    const float ge = w_of(I) * T;                                                \
+    float v = G[I] - omega_t * (G[I] - ge);                                      \
+    if (q > 0.0f) v += (w_of(I) * srcf) * q;                                     \
+    Pop<S>::st(Qo + p.plane[I], v, w_of(I) * Tb);                                \
+  }
+  XAC_FOR19(XAC_TCOLLIDE_S)
+#undef XAC_TCOLLIDE_S
+}
+
+// cells: the three class lists concatenated, each padded with kNoCell to a multiple of 512 so that every
+// block (<= 512 threads, a divisor of 512) sees one class. class_end: end of each class in the list.
+template <typename S, bool kMacro, bool kOwn>
+__global__ void __launch_bounds__(256) coupled_step_grouped_kernel(
+    const uint32_t* __restrict__ cells, uint32_t end_fluid, uint32_t end_solid, const S* __restrict__ Pin,
+    S* __restrict__ Pout, const S* __restrict__ Qin, S* __restrict__ Qout, const uint32_t* __restrict__ link,
+    const float* __restrict__ qsrc, const float* __restrict__ u_in_ptr, float* __restrict__ rho_o,
+    float* __restrict__ ux_o, float* __restrict__ uy_o, float* __restrict__ uz_o, const float* __restrict__ T0,
+    StepParams p) {
+  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t c = __ldg(cells + idx);
+  if (c == kNoCell) return;
+  const uint32_t lw = __ldg(link + c);
+  const uint32_t first = blockIdx.x * blockDim.x;
+  if (first < end_fluid) {
+    bulk_fluid_cell<S, kMacro, kOwn>(c, lw, Pin, Pout, Qin, Qout, qsrc, rho_o, ux_o, uy_o, uz_o, T0, p);
+  } else if (first < end_solid) {
+    bulk_solid_cell<S, kMacro, kOwn>(c, lw, Pout, Qin, Qout, qsrc, rho_o, ux_o, uy_o, uz_o, T0, p);
+  } else {
+    coupled_cell<S, kMacro, kOwn>(c, Pin, Pout, Qin, Qout, link, qsrc, u_in_ptr, rho_o, ux_o, uy_o, uz_o, T0, p,
+                                  true, lw, (lw & kFillBit) != 0u);
   }
 }
 

@@ -89,14 +89,15 @@ class Lattice:
         _capi.call("xac_lattice_steps_done", self._h, C.byref(v))
         return int(v.value)
 
-    def tune(self, block: int, cells_per_thread: int):
-        """Launch shape of the fused step (threads per block, cells per thread); results are unaffected."""
-        _capi.call("xac_lattice_tune", self._h, int(block), int(cells_per_thread))
+    def tune(self, block: int, variant: int):
+        """Launch shape of the fused step: threads per block and visiting order (0 memory order, 1 grouped by
+        cell class). Results are unaffected."""
+        _capi.call("xac_lattice_tune", self._h, int(block), int(variant))
 
     def get_tune(self):
-        b, c = C.c_int(), C.c_int()
-        _capi.call("xac_lattice_get_tune", self._h, C.byref(b), C.byref(c))
-        return int(b.value), int(c.value)
+        b, v = C.c_int(), C.c_int()
+        _capi.call("xac_lattice_get_tune", self._h, C.byref(b), C.byref(v))
+        return int(b.value), int(v.value)
 
     def set_inlet(self, u_in: float):
         with torch.cuda.device(self.device):
