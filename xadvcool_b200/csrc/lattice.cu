@@ -179,7 +179,7 @@ struct LatticeImpl {
   float relax[5] = {1.0f, 1.0f, 1.0f, 0.5f, 0.5f};  // omega_f, omega_tf, omega_ts, srcf_f, srcf_s (device-computed)
   float u_in_host = 0.0f;
   int tune_block = 128;  // threads per block of the step kernel
-  int tune_variant = 1;  // 0: cells in memory order; 1: cells grouped by class (bulk fluid / bulk solid / other)
+  int tune_variant = 0;  // 0: cells in memory order; 1: cells grouped by class (bulk fluid / bulk solid / other)
   uint32_t* cells = nullptr;                 // class-grouped cell list (kNoCell padding)
   uint32_t cells_len = 0, end_fluid = 0, end_solid = 0;
 
