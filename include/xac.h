@@ -241,6 +241,27 @@ typedef struct xac_run_result {
 
 int xac_lattice_run(xac_lattice *lat, const xac_run_opts *opts, xac_run_result *res, void *stream);
 
+/* ========================================================================== *
+ * Batch: many designs (uneven lattice sizes, one precision) advanced together by ONE persistent cooperative
+ * launch per `steps_per_launch` steps (captured in a CUDA graph where the driver allows it). Each design keeps
+ * the convergence test and divergence guard of src/simulation.py:123-156, evaluated on the device; converged
+ * and diverged designs retire and their share of the GPU goes to the others. No reference counterpart: the
+ * reference solves designs one after another (generate_dataset.py:365-436).
+ * ========================================================================== */
+typedef struct xac_batch xac_batch;
+int xac_batch_create(const xac_desc *designs, int n, xac_batch **out, void *stream);
+int xac_batch_destroy(xac_batch *batch);
+int xac_batch_size(const xac_batch *batch, int *n);
+/* The i-th design as a lattice owned by the batch: warm-start it (xac_lattice_init_fields) before a run, read
+ * fields / scalars / stats after. Do not destroy it. */
+int xac_batch_lattice(xac_batch *batch, int i, xac_lattice **lat);
+/* Threads per block (64, 128, 256; also the cells per tile) and steps per persistent launch. */
+int xac_batch_tune(xac_batch *batch, int block, int steps_per_launch);
+int xac_batch_get_tune(const xac_batch *batch, int *block, int *steps_per_launch);
+/* Run every design from step 0 to convergence, divergence or opts->max_steps (constant_power must be 0);
+ * results[i] receives design i's outcome. */
+int xac_batch_run(xac_batch *batch, const xac_run_opts *opts, xac_run_result *results, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

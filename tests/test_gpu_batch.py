@@ -1,0 +1,79 @@
+"""The persistent batched solve against solo solves of the same designs: identical step counts, convergence
+flags and fields (same kernels, same deterministic stats reduction)."""
+import numpy as np
+import pytest
+import torch
+
+from xadvcool_b200 import designs
+from xadvcool_b200.batch import Batch
+from xadvcool_b200.lattice import Lattice
+
+pytestmark = pytest.mark.gpu
+
+
+def small_designs():
+    out = []
+    for s, shape in enumerate([(40, 18, 10), (64, 24, 12), (52, 20, 9)]):
+        m, hs, u, info = designs.gyroid_design(s, nx=shape[0], ny=shape[1], nz=shape[2], buf=4)
+        out.append(dict(mask=m, heat_source=hs, tau_fluid=0.6 + 0.02 * s, u_inlet_val=min(u, 0.04), Pr=2.0,
+                        k_ratio=20.0, heat_power=0.02))
+    m = designs.straight_fin_plate()
+    out.append(dict(mask=m, tau_fluid=0.6, heat_power=1e-4, u_inlet_val=0.05, Pr=2.0, k_ratio=100.0))
+    return out
+
+
+def solo(d, **run):
+    lat = Lattice(d["mask"], **{k: v for k, v in d.items() if k != "mask"})
+    res = lat.run(**run)
+    f = [t.cpu().numpy() for t in lat.fields()]
+    lat.close()
+    return res, f
+
+
+@pytest.mark.parametrize("block,spl", [(128, 1000), (64, 250), (256, 7)])
+def test_batch_equals_solo_solves(block, spl, cuda):
+    ds = small_designs()
+    run = dict(max_steps=9000, stats_every=100, tol_ke=2e-4, tol_T=2e-4)
+    b = Batch(ds)
+    b.tune(block, spl)
+    res = b.run(**run)
+    for i, d in enumerate(ds):
+        ref, f_ref = solo(d, **run)
+        assert res[i]["steps"] == ref["steps"], (i, res[i]["steps"], ref["steps"])
+        assert res[i]["converged"] == ref["converged"] and res[i]["diverged"] == ref["diverged"]
+        assert res[i]["d_ke"] == ref["d_ke"]
+        f = [t.cpu().numpy() for t in b.lattice(i).fields()]
+        for a, c in zip(f, f_ref):
+            assert np.array_equal(a, c)
+    assert len({r["steps"] for r in res}) > 1  # designs retired at different steps
+
+
+def test_batch_divergence_retires_only_the_diverging_design(cuda):
+    ds = small_designs()[:2]
+    ds[1] = dict(ds[1], u_inlet_val=0.3, tau_fluid=0.51)
+    b = Batch(ds)
+    res = b.run(max_steps=3000, stats_every=100, tol_ke=0.0, tol_T=0.0)
+    assert res[1]["diverged"] and not res[0]["diverged"]
+    assert res[0]["steps"] == 3000 and res[1]["steps"] < 3000
+
+
+def test_batch_warm_start_and_fp16(cuda):
+    ds = small_designs()[:2]
+    b = Batch(ds, precision="fp16")
+    lat0 = b.lattice(0)
+    rho, u, T = lat0.fields()
+    lat0.init_fields(rho, u, T + 1.0)
+    res = b.run(max_steps=500, stats_every=100, tol_ke=0.0, tol_T=0.0)
+    assert all(r["steps"] == 500 for r in res)
+    s0 = b.lattice(0).stats()
+    assert np.isfinite(s0).all() and s0[16] == 0
+
+
+def test_batch_rejects_bad_input(cuda):
+    ds = small_designs()[:1]
+    b = Batch(ds)
+    with pytest.raises(Exception):
+        b.tune(100, 10)
+    b.run(max_steps=200, stats_every=100)
+    with pytest.raises(Exception):  # designs must restart from step 0
+        b.run(max_steps=200, stats_every=100)

@@ -105,6 +105,13 @@ SIGNATURES = {
     "xac_lattice_save_state": [_vp, _vp, C.c_size_t, _vp],
     "xac_lattice_load_state": [_vp, _vp, C.c_size_t, _vp],
     "xac_lattice_run": [_vp, C.POINTER(RunOpts), C.POINTER(RunResult), _vp],
+    "xac_batch_create": [C.POINTER(Desc), _i, C.POINTER(_vp), _vp],
+    "xac_batch_destroy": [_vp],
+    "xac_batch_size": [_vp, C.POINTER(_i)],
+    "xac_batch_lattice": [_vp, _i, C.POINTER(_vp)],
+    "xac_batch_tune": [_vp, _i, _i],
+    "xac_batch_get_tune": [_vp, C.POINTER(_i), C.POINTER(_i)],
+    "xac_batch_run": [_vp, C.POINTER(RunOpts), C.POINTER(RunResult), _vp],
 }
 
 _lib = None

@@ -8,6 +8,7 @@
 #include <utility>
 #include <vector>
 
+#include "batch.cuh"
 #include "lattice_kernels.cuh"
 #include "reductions.cuh"
 
@@ -374,10 +375,12 @@ struct LatticeImpl {
 };
 
 // ---------------------------------------------------------------- shared reduction drivers
-int run_stats(const FieldView& v, double* rows, int nblocks, double* dev_out, double* host_out, cudaStream_t s) {
+// rows must hold stats_tiles(cells) * kNStats doubles
+int run_stats(const FieldView& v, double* rows, double* dev_out, double* host_out, cudaStream_t s) {
   const auto spec = stats_spec();
-  stats_partials_kernel<<<nblocks, kBlock, 0, s>>>(v, spec, rows);
-  combine_rows_kernel<kNStats><<<1, 32 * kNStats, 0, s>>>(rows, nblocks, spec, dev_out);
+  const int ntiles = (int)stats_tiles((long long)v.nx * v.ny * v.nz);
+  stats_partials_kernel<<<ntiles, kStatsTile, 0, s>>>(v, spec, rows);
+  combine_rows_kernel<kNStats><<<1, 32 * kNStats, 0, s>>>(rows, ntiles, spec, dev_out);
   XAC_CUDA(cudaGetLastError());
   XAC_CUDA(cudaMemcpyAsync(host_out, dev_out, kNStats * sizeof(double), cudaMemcpyDeviceToHost, s));
   XAC_CUDA(cudaStreamSynchronize(s));
@@ -573,9 +576,10 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
   for (float** f : {&L.rho, &L.ux, &L.uy, &L.uz, &L.T})
     if ((r = dmalloc(f, n, "alloc fields")) != XAC_OK) return r;
   L.red_blocks = reduction_blocks(n);
-  if ((r = dmalloc(&L.rows, (size_t)L.red_blocks * (kNMetrics > kNStats ? kNMetrics : kNStats), "alloc rows")) !=
-      XAC_OK)
-    return r;
+  {
+    const size_t metric_rows = (size_t)L.red_blocks * kNMetrics, stat_rows = (size_t)stats_tiles(n) * kNStats;
+    if ((r = dmalloc(&L.rows, metric_rows > stat_rows ? metric_rows : stat_rows, "alloc rows")) != XAC_OK) return r;
+  }
   if ((r = dmalloc(&L.red_out, 64, "alloc red_out")) != XAC_OK) return r;
   XAC_CUDA(cudaMallocHost(&L.host_out, 64 * sizeof(double)));
   // the pop planes' padding is never read, but keep it defined
@@ -677,7 +681,7 @@ int xac_lattice_stats(xac_lattice* lat, double* out_host, void* stream) {
   cudaStream_t s = as_stream(stream);
   int r = L.finalize_T(s);
   if (r != XAC_OK) return r;
-  r = run_stats(L.view(), L.rows, L.red_blocks, L.red_out, L.host_out, s);
+  r = run_stats(L.view(), L.rows, L.red_out, L.host_out, s);
   if (r != XAC_OK) return r;
   std::memcpy(out_host, L.host_out, kNStats * sizeof(double));
   return XAC_OK;
@@ -896,11 +900,10 @@ int xac_stats_fields(const float* rho, const float* u, const float* T, const int
   XAC_REQUIRE(nx > 0 && ny > 0 && nz > 0, "xac_stats_fields: bad dimensions");
   cudaStream_t s = as_stream(stream);
   const long long n = (long long)nx * ny * nz;
-  const int nb = reduction_blocks(n);
   double* rows = nullptr;
   double* dout = nullptr;
   double* hout = nullptr;
-  int r = dmalloc(&rows, (size_t)nb * kNStats, "alloc rows");
+  int r = dmalloc(&rows, (size_t)stats_tiles(n) * kNStats, "alloc rows");
   if (r == XAC_OK) r = dmalloc(&dout, kNStats, "alloc out");
   if (r == XAC_OK && cudaMallocHost(&hout, kNStats * sizeof(double)) != cudaSuccess) r = XAC_ENOMEM;
   if (r == XAC_OK) {
@@ -919,7 +922,7 @@ int xac_stats_fields(const float* rho, const float* u, const float* T, const int
     v.nx = nx;
     v.ny = ny;
     v.nz = nz;
-    r = run_stats(v, rows, nb, dout, hout, s);
+    r = run_stats(v, rows, dout, hout, s);
     if (r == XAC_OK) std::memcpy(out_host, hout, kNStats * sizeof(double));
   }
   cudaFree(rows);
@@ -967,6 +970,281 @@ int xac_scalars_fields(const float* rho, const float* u, const float* T, const i
   cudaFree(dout);
   if (hout) cudaFreeHost(hout);
   return r;
+}
+
+}  // extern "C"
+
+// =====================================================================================================
+// Batch of designs advanced by one persistent cooperative launch (batch.cuh)
+// =====================================================================================================
+struct xac_batch {
+  std::vector<xac_lattice*> lats;
+  int precision = XAC_FP32;
+  int block = 128;              // threads per block (= cells per tile)
+  int steps_per_launch = 1000;  // steps one launch may advance
+  BatchDesign* dD = nullptr;
+  BatchCtl* dC = nullptr;
+  double* drows = nullptr;
+  size_t rows_cap = 0;
+  BatchCtl* hC = nullptr;  // pinned
+  std::vector<BatchDesign> hD;
+  std::map<std::pair<int, long long>, cudaGraphExec_t> graphs;
+  cudaStream_t capture = nullptr;
+  ~xac_batch() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    if (capture) cudaStreamDestroy(capture);
+    cudaFree(dD);
+    cudaFree(dC);
+    cudaFree(drows);
+    if (hC) cudaFreeHost(hC);
+    for (auto* l : lats) delete l;
+  }
+};
+
+namespace {
+
+template <typename S>
+int batch_launch(xac_batch* b, const BatchRun& run, cudaStream_t s, bool use_graph) {
+  int dev = 0, sms = 0, per_sm = 0;
+  XAC_CUDA(cudaGetDevice(&dev));
+  XAC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  XAC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_persistent_kernel<S>, b->block, 0));
+  XAC_REQUIRE(per_sm > 0, "xac_batch_run: the persistent kernel does not fit on an SM with %d threads", b->block);
+  const int grid = sms * per_sm;  // every block resident: the grid barrier cannot deadlock
+  BatchDesign* D = b->dD;
+  BatchCtl* C = b->dC;
+  double* rows = b->drows;
+  BatchRun r = run;
+  void* args[] = {&D, &C, &rows, &r};
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(b->block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (use_graph) {
+    auto key = std::make_pair(run.steps, run.max_steps);
+    auto it = b->graphs.find(key);
+    if (it == b->graphs.end()) {
+      if (!b->capture) XAC_CUDA(cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking));
+      cudaGraph_t graph = nullptr;
+      cfg.stream = b->capture;
+      XAC_CUDA(cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal));
+      cudaError_t le = cudaLaunchKernelExC(&cfg, (const void*)batch_persistent_kernel<S>, args);
+      cudaError_t ce = cudaStreamEndCapture(b->capture, &graph);
+      cudaGraphExec_t exec = nullptr;
+      if (le == cudaSuccess && ce == cudaSuccess && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+        cudaGraphDestroy(graph);
+        it = b->graphs.emplace(key, exec).first;
+      } else {
+        // the driver could not capture a cooperative launch: launch directly from now on
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        b->graphs.emplace(key, (cudaGraphExec_t) nullptr);
+        it = b->graphs.find(key);
+      }
+    }
+    if (it->second) {
+      XAC_CUDA(cudaGraphLaunch(it->second, s));
+      return XAC_OK;
+    }
+  }
+  cfg.stream = s;
+  XAC_CUDA(cudaLaunchKernelExC(&cfg, (const void*)batch_persistent_kernel<S>, args));
+  return XAC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int xac_batch_create(const xac_desc* descs, int n, xac_batch** out, void* stream) {
+  XAC_REQUIRE(out && descs, "xac_batch_create: null pointer");
+  XAC_REQUIRE(n >= 1 && n <= kMaxBatch, "xac_batch_create: batch size %d outside 1..%d", n, kMaxBatch);
+  *out = nullptr;
+  for (int i = 1; i < n; ++i)
+    XAC_REQUIRE(descs[i].precision == descs[0].precision, "xac_batch_create: designs must share one precision");
+  xac_batch* b = new (std::nothrow) xac_batch();
+  if (!b) {
+    set_error("xac_batch_create: host allocation failed");
+    return XAC_ENOMEM;
+  }
+  b->precision = descs[0].precision;
+  for (int i = 0; i < n; ++i) {
+    xac_lattice* l = nullptr;
+    int r = xac_lattice_create(&descs[i], &l, stream);
+    if (r != XAC_OK) {
+      delete b;
+      return r;
+    }
+    b->lats.push_back(l);
+  }
+  size_t rows = 0;
+  for (auto* l : b->lats) rows += (size_t)stats_tiles(l->impl.g.ncell);
+  b->rows_cap = rows;
+  int r = XAC_OK;
+  if ((r = dmalloc(&b->dD, (size_t)n, "alloc batch designs")) != XAC_OK ||
+      (r = dmalloc(&b->dC, 1, "alloc batch control")) != XAC_OK ||
+      (r = dmalloc(&b->drows, rows * kNStats, "alloc batch rows")) != XAC_OK) {
+    delete b;
+    return r;
+  }
+  if (cudaMallocHost(&b->hC, sizeof(BatchCtl)) != cudaSuccess) {
+    delete b;
+    set_error("xac_batch_create: pinned allocation failed");
+    return XAC_ENOMEM;
+  }
+  *out = b;
+  return XAC_OK;
+}
+
+int xac_batch_destroy(xac_batch* b) {
+  if (!b) return XAC_OK;
+  cudaDeviceSynchronize();
+  delete b;
+  return XAC_OK;
+}
+
+int xac_batch_size(const xac_batch* b, int* n) {
+  XAC_REQUIRE(b && n, "xac_batch_size: null pointer");
+  *n = (int)b->lats.size();
+  return XAC_OK;
+}
+
+int xac_batch_lattice(xac_batch* b, int i, xac_lattice** lat) {
+  XAC_REQUIRE(b && lat, "xac_batch_lattice: null pointer");
+  XAC_REQUIRE(i >= 0 && i < (int)b->lats.size(), "xac_batch_lattice: index %d out of range", i);
+  *lat = b->lats[i];
+  return XAC_OK;
+}
+
+int xac_batch_tune(xac_batch* b, int block, int steps_per_launch) {
+  XAC_REQUIRE(b, "xac_batch_tune: null batch");
+  XAC_REQUIRE(block == 64 || block == 128 || block == 256, "xac_batch_tune: block must be 64, 128 or 256");
+  XAC_REQUIRE(steps_per_launch >= 1, "xac_batch_tune: steps_per_launch must be positive");
+  if (b->block != block) {
+    for (auto& kv : b->graphs)
+      if (kv.second) cudaGraphExecDestroy(kv.second);
+    b->graphs.clear();
+  }
+  b->block = block;
+  b->steps_per_launch = steps_per_launch;
+  return XAC_OK;
+}
+
+int xac_batch_get_tune(const xac_batch* b, int* block, int* steps_per_launch) {
+  XAC_REQUIRE(b && block && steps_per_launch, "xac_batch_get_tune: null pointer");
+  *block = b->block;
+  *steps_per_launch = b->steps_per_launch;
+  return XAC_OK;
+}
+
+int xac_batch_run(xac_batch* b, const xac_run_opts* o, xac_run_result* res, void* stream) {
+  XAC_REQUIRE(b && o && res, "xac_batch_run: null pointer");
+  XAC_REQUIRE(o->stats_every > 0 && o->max_steps >= 0, "xac_batch_run: bad options");
+  XAC_REQUIRE(!o->constant_power, "xac_batch_run: the constant-power pump is run per lattice (xac_lattice_run)");
+  cudaStream_t s = as_stream(stream);
+  const int n = (int)b->lats.size();
+  b->hD.assign(n, BatchDesign{});
+  uint32_t row = 0;
+  for (int i = 0; i < n; ++i) {
+    LatticeImpl& L = b->lats[i]->impl;
+    XAC_REQUIRE(L.step == 0 && L.own_pending,
+                "xac_batch_run: design %d is not at step 0 (create it or re-initialise it with init_fields)", i);
+    BatchDesign& d = b->hD[i];
+    d.p = L.params();
+    d.P[0] = L.P[0];
+    d.P[1] = L.P[1];
+    d.Q[0] = L.Qb[0];
+    d.Q[1] = L.Qb[1];
+    d.link = L.link;
+    d.qsrc = L.qsrc;
+    d.u_in = L.u_in;
+    d.rho = L.rho;
+    d.ux = L.ux;
+    d.uy = L.uy;
+    d.uz = L.uz;
+    d.T = L.T;
+    d.ncell = (uint32_t)L.g.ncell;
+    d.tiles = (uint32_t)((L.g.ncell + b->block - 1) / b->block);
+    d.stat_tiles = (uint32_t)stats_tiles(L.g.ncell);
+    d.row_base = row;
+    row += d.stat_tiles;
+    const int a = (int)(0.6 * o->max_steps);
+    const double mu = L.u_inlet_nominal > 1e-6 ? L.u_inlet_nominal : 1e-6;
+    int bnd = (int)(2.0 * L.g.nx / mu);
+    if (bnd < 5000) bnd = 5000;
+    d.min_steps = a < bnd ? a : bnd;
+    d.active = 1;
+    d.dQ = 1.0;
+  }
+  std::memset(b->hC, 0, sizeof(BatchCtl));
+  uint32_t acc = 0, sacc = 0;
+  for (int i = 0; i < n; ++i) {
+    b->hC->active[i] = (uint32_t)i;
+    b->hC->prefix[i] = acc;
+    b->hC->stat_prefix[i] = sacc;
+    acc += b->hD[i].tiles;
+    sacc += b->hD[i].stat_tiles;
+  }
+  b->hC->prefix[n] = acc;
+  b->hC->stat_prefix[n] = sacc;
+  b->hC->n_active = n;
+  b->hC->all_done = n == 0 ? 1 : 0;
+  XAC_CUDA(cudaMemcpyAsync(b->dD, b->hD.data(), n * sizeof(BatchDesign), cudaMemcpyHostToDevice, s));
+  XAC_CUDA(cudaMemcpyAsync(b->dC, b->hC, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
+  BatchRun run{};
+  run.max_steps = o->max_steps;
+  run.stats_every = o->stats_every;
+  run.tol_ke = o->tol_ke;
+  run.tol_T = o->tol_T;
+  run.spin_limit = 1ull << 27;  // about 10 s of polling before a wait reports XAC_ETIMEOUT
+  long long done = 0;
+  while (done < o->max_steps && !b->hC->all_done) {
+    const long long left = o->max_steps - done;
+    run.steps = (int)(left < b->steps_per_launch ? left : b->steps_per_launch);
+    int r;
+    switch (b->precision) {
+      case XAC_FP16: r = batch_launch<__half>(b, run, s, true); break;
+      case XAC_BF16: r = batch_launch<__nv_bfloat16>(b, run, s, true); break;
+      default: r = batch_launch<float>(b, run, s, true);
+    }
+    if (r != XAC_OK) return r;
+    XAC_CUDA(cudaMemcpyAsync(b->hC, b->dC, 32, cudaMemcpyDeviceToHost, s));  // barrier words, err, done, step
+    XAC_CUDA(cudaStreamSynchronize(s));
+    if (b->hC->err) {
+      set_error("xac_batch_run: a grid-barrier wait gave up (device status %d)", b->hC->err);
+      return XAC_ETIMEOUT;
+    }
+    done = b->hC->step;
+  }
+  XAC_CUDA(cudaMemcpyAsync(b->hD.data(), b->dD, n * sizeof(BatchDesign), cudaMemcpyDeviceToHost, s));
+  XAC_CUDA(cudaStreamSynchronize(s));
+  for (int i = 0; i < n; ++i) {
+    const BatchDesign& d = b->hD[i];
+    xac_run_result& rr = res[i];
+    std::memset(&rr, 0, sizeof(rr));
+    const long long steps = d.active ? done : d.steps;
+    rr.steps = steps;
+    rr.diverged = d.diverged;
+    rr.converged = d.converged ? 1 : (!d.diverged && steps > d.min_steps && d.d_ke < o->tol_ke && d.dT < o->tol_T &&
+                                      d.dQ < o->tol_T);
+    rr.d_ke = d.d_ke;
+    rr.dT_conv = d.dT;
+    rr.dQ_conv = d.dQ;
+    rr.u_inlet_final = (double)b->lats[i]->impl.u_in_host;
+    std::memcpy(rr.last_stats, d.last, sizeof(d.last));
+    LatticeImpl& L = b->lats[i]->impl;
+    L.step = steps;
+    L.cur = (int)(steps & 1);
+    L.own_pending = steps == 0;
+    L.macro_step = steps;
+    L.T_step = (steps % o->stats_every == 0) ? steps : -1;
+  }
+  return XAC_OK;
 }
 
 }  // extern "C"

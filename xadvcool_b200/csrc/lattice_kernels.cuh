@@ -55,22 +55,31 @@ struct Geom {
 // FP32 stores the population itself. The 16-bit forms store the deviation from the rest
 // equilibrium w_i*ref (ref = 1 for the fluid, T_inlet for the thermal lattice) and do all
 // arithmetic in float32.
+// kCoherent loads go through L2 (ld.global.cg): needed when the data was written earlier in the same launch
+// (the persistent batch kernel); otherwise the read-only path (ld.global.nc) is used.
 template <typename S>
 struct Pop;
 template <>
 struct Pop<float> {
-  static __device__ __forceinline__ float ld(const float* p, float) { return __ldg(p); }
+  template <bool kCoherent = false>
+  static __device__ __forceinline__ float ld(const float* p, float) {
+    return kCoherent ? __ldcg(p) : __ldg(p);
+  }
   static __device__ __forceinline__ void st(float* p, float v, float) { *p = v; }
 };
 template <>
 struct Pop<__half> {
-  static __device__ __forceinline__ float ld(const __half* p, float base) { return __half2float(__ldg(p)) + base; }
+  template <bool kCoherent = false>
+  static __device__ __forceinline__ float ld(const __half* p, float base) {
+    return __half2float(kCoherent ? __ldcg(p) : __ldg(p)) + base;
+  }
   static __device__ __forceinline__ void st(__half* p, float v, float base) { *p = __float2half_rn(v - base); }
 };
 template <>
 struct Pop<__nv_bfloat16> {
+  template <bool kCoherent = false>
   static __device__ __forceinline__ float ld(const __nv_bfloat16* p, float base) {
-    return __bfloat162float(__ldg(p)) + base;
+    return __bfloat162float(kCoherent ? __ldcg(p) : __ldg(p)) + base;
   }
   static __device__ __forceinline__ void st(__nv_bfloat16* p, float v, float base) {
     *p = __float2bfloat16_rn(v - base);
@@ -107,7 +116,7 @@ __device__ __forceinline__ unsigned sector_group(int lane) {
 // fluid work: their fluid populations are the rest equilibrium w_i for ever (fluid_engine3d.py:193-194 never
 // streams them, and they start at rho=1, u=0); a solid lane still stores w_i when a fluid lane shares its
 // sector, so every sector of the fluid output is written whole.
-template <typename S, bool kMacro, bool kOwn>
+template <typename S, bool kMacro, bool kOwn, bool kCoherent = false>
 __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restrict__ Pin, S* __restrict__ Pout,
                                              const S* __restrict__ Qin, S* __restrict__ Qout,
                                              const uint32_t* __restrict__ link, const float* __restrict__ qsrc,
@@ -131,7 +140,7 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
     if (type == kInlet) {
       // src/fluid_engine3d.py:197-244: no pull; unknown populations from the known ones
       float k[kQ];
-#define XAC_LD_OWN(I) k[I] = Pop<S>::ld(Pc + p.plane[I], w_of(I));
+#define XAC_LD_OWN(I) k[I] = Pop<S>::template ld<kCoherent>(Pc + p.plane[I], w_of(I));
       XAC_FOR19(XAC_LD_OWN)
 #undef XAC_LD_OWN
       const float ux_in = __ldg(u_in_ptr);
@@ -163,7 +172,7 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
       const S* __restrict__ Ps = (lw & kXLoBit) ? Pc : Pc - 1;
       float sum = 0.0f;
 #define XAC_LD_OUT(I)                              \
-  F[I] = Pop<S>::ld(Ps + p.plane[I], w_of(I));     \
+  F[I] = Pop<S>::template ld<kCoherent>(Ps + p.plane[I], w_of(I));     \
   sum += F[I];
       XAC_FOR19(XAC_LD_OUT)
 #undef XAC_LD_OUT
@@ -175,7 +184,7 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
     } else {
       // src/fluid_engine3d.py:262-272: pull, halfway bounce-back on out-of-domain or solid sources
 #define XAC_LD_PULL(I)                                                                                      \
-  F[I] = ((lw >> I) & 1u) ? Pop<S>::ld(Pc + p.plane[opp_of(I)], w_of(I)) : Pop<S>::ld(Pc + p.pull[I], w_of(I));
+  F[I] = ((lw >> I) & 1u) ? Pop<S>::template ld<kCoherent>(Pc + p.plane[opp_of(I)], w_of(I)) : Pop<S>::template ld<kCoherent>(Pc + p.pull[I], w_of(I));
       XAC_FOR19(XAC_LD_PULL)
 #undef XAC_LD_PULL
     }
@@ -215,7 +224,7 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
       float r = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f;
 #pragma unroll
       for (int i = 0; i < kQ; ++i) {
-        const float v = Pop<S>::ld(Pc + p.plane[i], w_of(i));
+        const float v = Pop<S>::template ld<kCoherent>(Pc + p.plane[i], w_of(i));
         r += v;
         if (ex_of(i) != 0) mx += ex_of(i) > 0 ? v : -v;
         if (ey_of(i) != 0) my += ey_of(i) > 0 ? v : -v;
@@ -238,10 +247,10 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
   float G[kQ];
   float T;
   if (kOwn) {
-#define XAC_LD_G0(I) G[I] = Pop<S>::ld(Qc + p.plane[I], w_of(I) * Tb);
+#define XAC_LD_G0(I) G[I] = Pop<S>::template ld<kCoherent>(Qc + p.plane[I], w_of(I) * Tb);
     XAC_FOR19(XAC_LD_G0)
 #undef XAC_LD_G0
-    T = __ldg(T0 + c);
+    T = kCoherent ? __ldcg(T0 + c) : __ldg(T0 + c);
   } else {
     if (type == kInlet) {
       // src/thermal_engine3d.py:160-165
@@ -250,7 +259,7 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
     } else if (type == kOutlet) {
       // src/thermal_engine3d.py:170-177
       const S* __restrict__ Qs = (lw & kXLoBit) ? Qc : Qc - 1;
-#define XAC_LD_GOUT(I) G[I] = Pop<S>::ld(Qs + p.plane[I], w_of(I) * Tb);
+#define XAC_LD_GOUT(I) G[I] = Pop<S>::template ld<kCoherent>(Qs + p.plane[I], w_of(I) * Tb);
       XAC_FOR19(XAC_LD_GOUT)
 #undef XAC_LD_GOUT
     } else if (!(lw & kYZBit)) {
@@ -259,11 +268,11 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
 #define XAC_LD_GFAST(I)                                                                                        \
   {                                                                                                            \
     if (ex_of(I) == 1)                                                                                         \
-      G[I] = (lw & kXLoBit) ? w_of(I) * p.T_in : Pop<S>::ld(Qc + p.pull[I], w_of(I) * Tb);                     \
+      G[I] = (lw & kXLoBit) ? w_of(I) * p.T_in : Pop<S>::template ld<kCoherent>(Qc + p.pull[I], w_of(I) * Tb);                     \
     else if (ex_of(I) == -1)                                                                                   \
-      G[I] = (lw & kXHiBit) ? Pop<S>::ld(Qc + p.plane[I], w_of(I) * Tb) : Pop<S>::ld(Qc + p.pull[I], w_of(I) * Tb); \
+      G[I] = (lw & kXHiBit) ? Pop<S>::template ld<kCoherent>(Qc + p.plane[I], w_of(I) * Tb) : Pop<S>::template ld<kCoherent>(Qc + p.pull[I], w_of(I) * Tb); \
     else                                                                                                       \
-      G[I] = Pop<S>::ld(Qc + p.pull[I], w_of(I) * Tb);                                                         \
+      G[I] = Pop<S>::template ld<kCoherent>(Qc + p.pull[I], w_of(I) * Tb);                                                         \
   }
       XAC_FOR19(XAC_LD_GFAST)
 #undef XAC_LD_GFAST
@@ -277,11 +286,11 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
     if (xlo)                                                                                                   \
       G[I] = w_of(I) * p.T_in;                                                                                 \
     else if (xhi)                                                                                              \
-      G[I] = Pop<S>::ld(Qc + p.plane[I], w_of(I) * Tb);                                                        \
+      G[I] = Pop<S>::template ld<kCoherent>(Qc + p.plane[I], w_of(I) * Tb);                                                        \
     else if (wall)                                                                                             \
-      G[I] = Pop<S>::ld(Qc + p.plane[opp_of(I)], w_of(I) * Tb);                                                \
+      G[I] = Pop<S>::template ld<kCoherent>(Qc + p.plane[opp_of(I)], w_of(I) * Tb);                                                \
     else                                                                                                       \
-      G[I] = Pop<S>::ld(Qc + p.pull[I], w_of(I) * Tb);                                                         \
+      G[I] = Pop<S>::template ld<kCoherent>(Qc + p.pull[I], w_of(I) * Tb);                                                         \
   }
       XAC_FOR19(XAC_LD_GSLOW)
 #undef XAC_LD_GSLOW

@@ -91,50 +91,85 @@ inline ReduceSpec<kNStats> stats_spec() {
   return s;
 }
 
+// Stats of one cell added into acc (XAC_ST_* slots). Field reads go through L2 (they may have been written
+// earlier in the same launch by other blocks).
+__device__ __forceinline__ void stats_accumulate(const FieldView& v, int x, int y, int z, double (&acc)[kNStats]) {
+  const long long cell = x * v.sx + y * v.sy + z * v.sz;
+  const int m = view_type(v, cell);
+  const float ux = __ldcg(v.ux + cell * v.ustride), uy = __ldcg(v.uy + cell * v.ustride),
+              uz = __ldcg(v.uz + cell * v.ustride);
+  const float vsq = (ux * ux + uy * uy) + uz * uz;
+  const float vmag = sqrtf(vsq);
+  const float r = __ldcg(v.rho + cell), T = __ldcg(v.T + cell);
+  if (!isfinite(vmag) || !isfinite(T)) acc[XAC_ST_NONFINITE] += 1.0;
+  acc[XAC_ST_SUM_KE] += (double)vsq;
+  if (m != kSolid) {
+    acc[XAC_ST_MAX_V] = fmax(acc[XAC_ST_MAX_V], (double)vmag);
+    acc[XAC_ST_SUM_V] += (double)vmag;
+    acc[XAC_ST_COUNT] += 1.0;
+    acc[XAC_ST_SUM_RHO] += (double)r;
+  }
+  if (x == 1) {
+    acc[XAC_ST_SUM_RHO_IN] += (double)r;
+    acc[XAC_ST_C_IN] += 1.0;
+  }
+  if (x == v.nx - 2) {
+    acc[XAC_ST_SUM_RHO_OUT] += (double)r;
+    acc[XAC_ST_C_OUT] += 1.0;
+  }
+  if (m == kOutlet) {
+    acc[XAC_ST_SUM_UX_OUT] += (double)ux;
+    acc[XAC_ST_C_OUTLET] += 1.0;
+    acc[XAC_ST_Q_OUT] += (double)(ux * T);
+    acc[XAC_ST_Q_OUT_COUNT] += 1.0;
+  }
+  acc[XAC_ST_MAX_T] = fmax(acc[XAC_ST_MAX_T], (double)T);
+  acc[XAC_ST_SUM_T] += (double)T;
+  acc[XAC_ST_COUNT_T] += 1.0;
+}
+
+// One row of partial stats for the 256-cell tile `tile` (cells enumerated x fastest). The tile is reduced as 8
+// chunks of 32 cells, each by one warp with a fixed butterfly, and the chunks are combined in order by one
+// thread: the row does not depend on the block size that computes it. Every thread of the block must call.
+constexpr int kStatsTile = 256;
+__device__ __forceinline__ void stats_tile_row(const FieldView& v, long long tile, const ReduceSpec<kNStats>& spec,
+                                               double* __restrict__ row) {
+  __shared__ double chunk[kStatsTile / 32][kNStats];
+  const long long n = (long long)v.nx * v.ny * v.nz;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int ch = warp; ch < kStatsTile / 32; ch += nwarps) {
+    double acc[kNStats];
+#pragma unroll
+    for (int k = 0; k < kNStats; ++k) acc[k] = identity(spec.op[k]);
+    const long long i = tile * kStatsTile + ch * 32 + lane;
+    if (i < n) {
+      const int x = (int)(i % v.nx);
+      const long long t = i / v.nx;
+      stats_accumulate(v, x, (int)(t % v.ny), (int)(t / v.ny), acc);
+    }
+#pragma unroll
+    for (int k = 0; k < kNStats; ++k) {
+      double a = acc[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) a = combine(spec.op[k], a, __shfl_xor_sync(0xffffffffu, a, o));
+      if (lane == 0) chunk[ch][k] = a;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < kNStats) {
+    const int k = threadIdx.x;
+    double a = identity(spec.op[k]);
+    for (int ch = 0; ch < kStatsTile / 32; ++ch) a = combine(spec.op[k], a, chunk[ch][k]);
+    row[k] = a;
+  }
+  __syncthreads();
+}
+
+inline long long stats_tiles(long long ncell) { return (ncell + kStatsTile - 1) / kStatsTile; }
+
 __global__ void __launch_bounds__(256) stats_partials_kernel(FieldView v, ReduceSpec<kNStats> spec,
                                                              double* __restrict__ rows) {
-  double acc[kNStats];
-#pragma unroll
-  for (int k = 0; k < kNStats; ++k) acc[k] = identity(spec.op[k]);
-  const long long n = (long long)v.nx * v.ny * v.nz;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    // i enumerates cells x fastest; any order gives the same sums up to FP64 rounding
-    const int x = (int)(i % v.nx);
-    const long long t = i / v.nx;
-    const int y = (int)(t % v.ny), z = (int)(t / v.ny);
-    const long long cell = x * v.sx + y * v.sy + z * v.sz;
-    const int m = view_type(v, cell);
-    const float ux = v.ux[cell * v.ustride], uy = v.uy[cell * v.ustride], uz = v.uz[cell * v.ustride];
-    const float vsq = (ux * ux + uy * uy) + uz * uz;
-    const float vmag = sqrtf(vsq);
-    const float r = v.rho[cell], T = v.T[cell];
-    if (!isfinite(vmag) || !isfinite(T)) acc[XAC_ST_NONFINITE] += 1.0;
-    acc[XAC_ST_SUM_KE] += (double)vsq;
-    if (m != kSolid) {
-      acc[XAC_ST_MAX_V] = fmax(acc[XAC_ST_MAX_V], (double)vmag);
-      acc[XAC_ST_SUM_V] += (double)vmag;
-      acc[XAC_ST_COUNT] += 1.0;
-      acc[XAC_ST_SUM_RHO] += (double)r;
-    }
-    if (x == 1) {
-      acc[XAC_ST_SUM_RHO_IN] += (double)r;
-      acc[XAC_ST_C_IN] += 1.0;
-    }
-    if (x == v.nx - 2) {
-      acc[XAC_ST_SUM_RHO_OUT] += (double)r;
-      acc[XAC_ST_C_OUT] += 1.0;
-    }
-    if (m == kOutlet) {
-      acc[XAC_ST_SUM_UX_OUT] += (double)ux;
-      acc[XAC_ST_C_OUTLET] += 1.0;
-      acc[XAC_ST_Q_OUT] += (double)(ux * T);
-      acc[XAC_ST_Q_OUT_COUNT] += 1.0;
-    }
-    acc[XAC_ST_MAX_T] = fmax(acc[XAC_ST_MAX_T], (double)T);
-    acc[XAC_ST_SUM_T] += (double)T;
-    acc[XAC_ST_COUNT_T] += 1.0;
-  }
-  block_reduce<kNStats>(acc, spec, rows + (long long)blockIdx.x * kNStats);
+  stats_tile_row(v, blockIdx.x, spec, rows + (long long)blockIdx.x * kNStats);
 }
 
 // ---- scalar metrics (generate_dataset.py:57-179) ------------------------------------------------

@@ -51,11 +51,23 @@ class Lattice:
             _capi.call("xac_lattice_create", C.byref(d), C.byref(self._h), stream_ptr(self.device))
         self.mask = mask_np
 
+    @classmethod
+    def _borrowed(cls, handle, mask, params, device):
+        """A view of a lattice owned by someone else (a batch): never destroyed from here."""
+        self = cls.__new__(cls)
+        self._h = C.c_void_p(handle)
+        self._owner = False
+        self.mask = np.ascontiguousarray(mask, dtype=np.int32)
+        self.shape = self.mask.shape
+        self.params = dict(params)
+        self.device = torch.device(device)
+        return self
+
     # -- lifecycle -------------------------------------------------------------------------------
     def close(self):
-        if getattr(self, "_h", None) is not None and self._h.value:
+        if getattr(self, "_owner", True) and getattr(self, "_h", None) is not None and self._h.value:
             _capi.load().xac_lattice_destroy(self._h)
-            self._h = C.c_void_p()
+        self._h = C.c_void_p()
 
     def __del__(self):
         try:
