@@ -141,7 +141,10 @@ struct BatchRun {
 };
 
 template <typename S>
-__global__ void __launch_bounds__(256) batch_persistent_kernel(BatchDesign* __restrict__ D, BatchCtl* __restrict__ ctl,
+#ifndef XAC_BATCH_MIN_BLOCKS
+#define XAC_BATCH_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(256, XAC_BATCH_MIN_BLOCKS) batch_persistent_kernel(BatchDesign* __restrict__ D, BatchCtl* __restrict__ ctl,
                                                                double* __restrict__ rows, BatchRun run) {
   __shared__ double st[kNStats];
   ReduceSpec<kNStats> spec;
