@@ -121,6 +121,15 @@ int xac_stream(const float *f_post, float *f_streamed, const int32_t *mask, cons
  * the call synchronises `stream`. */
 int xac_stats_fields(const float *rho, const float *u, const float *T, const int32_t *mask, int nx, int ny, int nz,
                      double *out_host, void *stream);
+/* No counterpart in the reference. The same stats as xac_stats_fields for callers that cannot allocate device or
+ * pinned memory (code running inside a stream capture, or under a memory budget owned by another allocator):
+ * it calls no allocator. Its scratch is a fixed 1.1 MB array in the library's device image, held by every GPU
+ * that loads the library; lattices above 2,097,152 cells are rejected (XAC_EINVAL). The result (XAC_NSTATS
+ * doubles) goes to the caller's DEVICE buffer out_dev, asynchronously on `stream`. All calls on a device share
+ * the scratch, so calls whose GPU work overlaps race. The first call on a device looks up the scratch address;
+ * make it before any stream capture. */
+int xac_stats_fields_noalloc(const float *rho, const float *u, const float *T, const int32_t *mask, int nx, int ny,
+                             int nz, double *out_dev, void *stream);
 
 /* src/thermal_engine3d.py:7-47 compute_thermal_equilibrium_kernel(rho, u, T, g_eq, mask) (rho unused, as there) */
 int xac_thermal_equilibrium(const float *u, const float *T, float *g_eq, const int32_t *mask, int nx, int ny, int nz,

@@ -78,6 +78,7 @@ SIGNATURES = {
     "xac_fused_collision": [_vp, _vp, _vp, _vp, _vp, _f, _i, _i, _i, _vp],
     "xac_stream": [_vp, _vp, _vp, _vp, _f, _i, _i, _i, _vp],
     "xac_stats_fields": [_vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp],
+    "xac_stats_fields_noalloc": [_vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp],
     "xac_thermal_equilibrium": [_vp, _vp, _vp, _vp, _i, _i, _i, _vp],
     "xac_thermal_bgk_collision": [_vp, _vp, _vp, _vp, _f, _f, _vp, _f, _i, _i, _i, _vp],
     "xac_fused_thermal_collision": [_vp, _vp, _vp, _vp, _vp, _f, _f, _vp, _f, _i, _i, _i, _vp],

@@ -24,6 +24,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "--expt-r
 UNITS = [
     ("ops_reference_layout.cu", ["--fmad=false"]),
     ("lattice.cu", ["--fmad=false"]),
+    ("stats_noalloc.cu", ["--fmad=false"]),
 ]
 
 

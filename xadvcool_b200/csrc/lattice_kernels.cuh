@@ -503,7 +503,7 @@ __global__ void __launch_bounds__(256) coupled_step_grouped_kernel(
 }
 
 // omega and source factors, computed with the device's IEEE division once per lattice
-__global__ void relaxation_factors_kernel(float tau_f, float tau_tf, float tau_ts, float* out) {
+static __global__ void relaxation_factors_kernel(float tau_f, float tau_tf, float tau_ts, float* out) {
   const float of = 1.0f / tau_f, otf = 1.0f / tau_tf, ots = 1.0f / tau_ts;
   out[0] = of;
   out[1] = otf;

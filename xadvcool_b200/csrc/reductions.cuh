@@ -167,7 +167,7 @@ __device__ __forceinline__ void stats_tile_row(const FieldView& v, long long til
 
 inline long long stats_tiles(long long ncell) { return (ncell + kStatsTile - 1) / kStatsTile; }
 
-__global__ void __launch_bounds__(256) stats_partials_kernel(FieldView v, ReduceSpec<kNStats> spec,
+static __global__ void __launch_bounds__(256) stats_partials_kernel(FieldView v, ReduceSpec<kNStats> spec,
                                                              double* __restrict__ rows) {
   stats_tile_row(v, blockIdx.x, spec, rows + (long long)blockIdx.x * kNStats);
 }
@@ -212,7 +212,7 @@ struct MetricBox {
   int buf, core_nx, core_ny;
 };
 
-__global__ void __launch_bounds__(256) metric_partials_kernel(FieldView v, MetricBox b, ReduceSpec<kNMetrics> spec,
+static __global__ void __launch_bounds__(256) metric_partials_kernel(FieldView v, MetricBox b, ReduceSpec<kNMetrics> spec,
                                                               double* __restrict__ rows) {
   double acc[kNMetrics];
 #pragma unroll
