@@ -231,6 +231,37 @@ def run_reference_arm(args):
 
 
 # ------------------------------------------------------------------------------------------------ GPU
+def forms_probe(dev, mask, lat_kw, shape):
+    """Side measurements of the other forms on the same GPU (outside the timed region): FP16 / BF16 population
+    storage on the same design, and the persistent batched solve of 64 mixed designs (1000 steps)."""
+    import torch
+    from xadvcool_b200 import autotune, designs
+    from xadvcool_b200.batch import Batch
+    from xadvcool_b200.lattice import Lattice
+    out = {}
+    for prec in ("fp16", "bf16"):
+        lat = Lattice(mask, device=dev, precision=prec, **lat_kw)
+        lat.step(2)
+        us = autotune.time_config(lat, shape["block"], shape["variant"], steps=200, repeats=3)
+        out[f"{prec}_mlups"] = round(mask.size / us, 1)
+        lat.close()
+    ds = []
+    for s in range(64):
+        m, h, u, _ = designs.mixed_design(s)
+        ds.append(dict(mask=m, heat_source=h, tau_fluid=0.56, u_inlet_val=u))
+    cells = sum(d["mask"].size for d in ds)
+    b = Batch(ds, device=dev)
+    torch.cuda.synchronize(dev)
+    t = time.perf_counter()
+    b.run(max_steps=1000, stats_every=100, tol_ke=0.0, tol_T=0.0)
+    torch.cuda.synchronize(dev)
+    dt = time.perf_counter() - t
+    b.close()
+    out["batch64_mixed_mlups"] = round(cells * 1000 / dt / 1e6, 1)
+    out["batch64_cells"] = cells
+    return out
+
+
 def run_gpu_arm(args):
     import torch
     rank, world, local = dist_init(args.gpus)
@@ -242,8 +273,11 @@ def run_gpu_arm(args):
     mask, hs, u_in, info = workload(rank)
     cells = mask.size
     n_solid = int((mask == 1).sum())
-    lat = Lattice(mask, heat_source=hs, tau_fluid=TAU, heat_power=POWER, u_inlet_val=u_in, Pr=PR,
-                  k_ratio=K_RATIO, device=dev)
+    lat_kw = dict(heat_source=hs, tau_fluid=TAU, heat_power=POWER, u_inlet_val=u_in, Pr=PR, k_ratio=K_RATIO)
+    from xadvcool_b200 import autotune
+    shape = autotune.autotune(mask, device=dev, lattice_kwargs=lat_kw)  # scratch lattice; cached per design
+    lat = Lattice(mask, device=dev, **lat_kw)
+    lat.tune(shape["block"], shape["variant"])
     stream = torch.cuda.current_stream(dev)
 
     def bench_step(ev=None):
@@ -284,6 +318,7 @@ def run_gpu_arm(args):
     peak, peak_kind = hbm_peak()
     tpc = ncu_traffic_per_cell()
     lat.close()
+    forms = forms_probe(dev, mask, lat_kw, shape) if rank == 0 else None
 
     # e2e: a full solve through the public API, host numpy in and out
     barrier(world)
@@ -321,6 +356,8 @@ def run_gpu_arm(args):
                         "d2h_bytes_per_step": d2h, "s_per_converged_design": round(e2e_max, 4),
                         "solver_steps": res["steps"], "converged": res["converged"]},
                 "gpu_launches": args.steps * (STEPS_PER_BENCH_STEP + 3),
+                "launch_shape": {"block": shape["block"], "variant": shape["variant"], "autotuned": shape["table"]},
+                "forms": forms,
                 "clocks": clk.summary(),
                 "last_stats": {"max_v": float(st[0]), "max_T": float(st[11])}}
         if cpu:
