@@ -300,11 +300,13 @@ def run_gpu_arm(args):
     barrier(world)
     torch.cuda.synchronize(dev)
     with ClockSampler(uuid) as clk:
+        torch.cuda.nvtx.range_push("timed")  # profilers can filter on this range
         t0.record(stream)
         for k in range(args.steps):
             st = bench_step(evs[k])
         t1.record(stream)
         torch.cuda.synchronize(dev)
+        torch.cuda.nvtx.range_pop()
     barrier(world)
     ms = t0.elapsed_time(t1)
     step_ms = sum(a.elapsed_time(b) for a, b in evs) / (args.steps * STEPS_PER_BENCH_STEP)
