@@ -225,3 +225,19 @@ def test_tune_rejects_bad_shapes(cuda):
         lat.tune(96, 0)
     with pytest.raises(Exception):
         lat.tune(128, 2)
+
+
+def test_autotune_picks_a_valid_shape_without_touching_results(cuda, tmp_path, monkeypatch):
+    from xadvcool_b200 import autotune
+    monkeypatch.setenv("XAC_AUTOTUNE_CACHE", str(tmp_path / "cache.json"))
+    mask, hs, u_in, _ = designs.gyroid_design(2, nx=40, ny=16, nz=10)
+    kw = dict(heat_source=hs, tau_fluid=0.57, u_inlet_val=u_in)
+    res = autotune.autotune(mask, steps=20, lattice_kwargs=kw)
+    assert res["block"] in autotune.BLOCKS and res["variant"] in autotune.VARIANTS
+    assert len(res["table"]) == len(autotune.BLOCKS) * len(autotune.VARIANTS)
+    assert autotune.autotune(mask, steps=20, lattice_kwargs=kw) == res  # cached
+    lat = Lattice(mask, **kw)
+    autotune.apply(lat, steps=20, lattice_kwargs=kw)
+    lat.step(30)
+    ref = oracle_fields(mask, 30, hs=hs, tau_fluid=0.57, u_inlet_val=u_in)
+    assert_exact(ref, *[t.cpu().numpy() for t in lat.fields()])

@@ -73,8 +73,10 @@ def autotune(mask, *, heat_source=None, precision="fp32", device="cuda", steps=1
     if key in cache:
         return cache[key]
     kw = dict(lattice_kwargs or {})
+    if heat_source is not None or "heat_source" not in kw:
+        kw["heat_source"] = heat_source
     table = {}
-    with Lattice(mask, heat_source=heat_source, precision=precision, device=dev, **kw) as scratch:
+    with Lattice(mask, precision=precision, device=dev, **kw) as scratch:
         scratch.step(2)
         for b in BLOCKS:
             for v in VARIANTS:
