@@ -74,7 +74,19 @@ __global__ void combine_rows_kernel(const double* __restrict__ rows, int nrows, 
   if (k >= K) return;
   const int op = spec.op[k];
   double v = identity(op);
-  for (int r = lane; r < nrows; r += 32) v = combine(op, v, rows[(long long)r * K + k]);
+  // a lane combines rows lane, lane+32, lane+64, ... in that order; eight loads are issued before they are
+  // combined, which hides their latency without changing the order
+  for (int r0 = lane; r0 < nrows; r0 += 32 * 8) {
+    double t[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int r = r0 + 32 * j;
+      t[j] = r < nrows ? rows[(long long)r * K + k] : identity(op);
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (r0 + 32 * j < nrows) v = combine(op, v, t[j]);
+  }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = combine(op, v, __shfl_down_sync(0xffffffffu, v, o));
   if (lane == 0) out[k] = v;
@@ -142,10 +154,10 @@ __device__ __forceinline__ void stats_tile_row(const FieldView& v, long long til
 #pragma unroll
     for (int k = 0; k < kNStats; ++k) acc[k] = identity(spec.op[k]);
     const long long i = tile * kStatsTile + ch * 32 + lane;
-    if (i < n) {
-      const int x = (int)(i % v.nx);
-      const long long t = i / v.nx;
-      stats_accumulate(v, x, (int)(t % v.ny), (int)(t / v.ny), acc);
+    if (i < n) {  // lattices stay below 2^31 cells: 32-bit decomposition
+      const unsigned iu = (unsigned)i, nx = (unsigned)v.nx, ny = (unsigned)v.ny;
+      const unsigned t = iu / nx;
+      stats_accumulate(v, (int)(iu - t * nx), (int)(t % ny), (int)(t / ny), acc);
     }
 #pragma unroll
     for (int k = 0; k < kNStats; ++k) {
