@@ -238,6 +238,8 @@ typedef struct xac_run_opts {
     double tol_ke, tol_T; /* relative-rate thresholds                   */
     int constant_power;   /* 0: constant_flow, 1: constant_power pump   */
     double target_power;
+    int min_steps;        /* 0: the reference's rule, no convergence before min(0.6 max_steps, max(5000, 2 nx / u_in))
+                           * steps (src/simulation.py:102-104); > 0: that many steps instead (warm starts)            */
 } xac_run_opts;
 
 typedef struct xac_run_result {
@@ -249,6 +251,23 @@ typedef struct xac_run_result {
 } xac_run_result;
 
 int xac_lattice_run(xac_lattice *lat, const xac_run_opts *opts, xac_run_result *res, void *stream);
+
+/* ========================================================================== *
+ * Warm-start surrogate convolutions: BF16 tensor-core implicit GEMMs (mma.sync m16n8k16), FP32 accumulation.
+ * Activations channels-last [N][D][H][W][C] BF16 (DEVICE pointers); weights [taps][Co][Ci] BF16 with
+ * taps = 27 (3x3x3, tap = (dz+1)*9 + (dy+1)*3 + (dx+1)) or 1; zero padding; Ci, Co multiples of 16
+ * (Ci, Co <= 256). No reference counterpart: the reference's surrogates run through cuDNN
+ * (benchmark/models/unet3d.py:11-125).
+ * ========================================================================== */
+/* out = act(bias + conv(in, w)); activation 0 = none, 1 = GELU; exactly one of out_bf16 / out_f32. The data
+ * gradient is this call on d_out with weights w'[26 - tap][ci][co] = w[tap][co][ci]. */
+int xac_conv3d_forward(const void *in, int N, int D, int H, int W, int Ci, const void *weight, const float *bias,
+                       int Co, int ksize, int activation, void *out_bf16, float *out_f32, void *stream);
+/* dw[tap][co][ci] = sum_v d_out[v][co] in[v + off(tap)][ci] (FP32), db[co] = sum_v d_out[v][co] (db may be NULL);
+ * partial: xac_conv3d_partial_floats() floats of device scratch. Deterministic (fixed reduction order). */
+int xac_conv3d_weight_grad(const void *in, int N, int D, int H, int W, int Ci, const void *d_out, int Co, int ksize,
+                           float *partial, float *dw, float *db, void *stream);
+int xac_conv3d_partial_floats(int N, int D, int H, int W, int Ci, int Co, int ksize, long long *count);
 
 /* ========================================================================== *
  * Batch: many designs (uneven lattice sizes, one precision) advanced together by ONE persistent cooperative

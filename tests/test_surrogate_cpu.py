@@ -1,0 +1,76 @@
+"""Host-side logic of the warm-start surrogate on the CPU, with torch's conv3d standing in for the tensor-core
+kernels: network shapes, the training loop, the adjoint-weight identity the data gradient relies on, and the
+mapping between solver fields and the network's channels-last targets."""
+import numpy as np
+import torch
+import torch.nn.functional as F
+
+from xadvcool_b200 import surrogate as S
+from xadvcool_b200.designs import gyroid_design
+
+
+def test_forward_shapes_cpu():
+    m = S.Surrogate("cpu", seed=0)
+    x = torch.randn(2, 8, 16, 24, 16).to(S.BF16)
+    y = m.forward(x, S.torch_conv3d)
+    assert y.shape == (2, 8, 16, 24, 16) and y.dtype == torch.float32
+    assert torch.isfinite(y).all()
+    # padded output channels stay exactly zero (zero weights and bias)
+    assert (y[..., S.OUT_FIELDS:] == 0).all()
+
+
+def test_training_loop_reduces_loss_cpu():
+    torch.manual_seed(0)
+    m = S.Surrogate("cpu", seed=1)
+    x = torch.zeros(1, 8, 16, 24, 16)
+    x[..., 0] = (torch.rand(1, 8, 16, 24) > 0.4).float()
+    x[..., 1] = torch.rand(1, 8, 16, 24)
+    x = x.to(S.BF16)
+    y = torch.zeros(1, 8, 16, 24, S.OUT_FIELDS)
+    y[..., 0] = x[..., 0].float() * (1 + x[..., 1].float())
+    y[..., 4] = x[..., 1].float() ** 2
+    hist = S.train(m, [(x, y)], epochs=40, batch=1, lr=3e-3, conv=S.torch_conv3d)
+    assert np.isfinite(hist).all()
+    assert hist[-1] < 0.3 * hist[0], hist
+
+
+def test_adjoint_weights_give_data_gradient():
+    """conv(dy, adjoint(w)) is the gradient of <conv(x, w), dy> with respect to x (zero padding)."""
+    g = torch.Generator().manual_seed(2)
+    x = torch.randn(1, 4, 5, 6, 16, generator=g).to(S.BF16).float().requires_grad_(True)
+    w = torch.randn(27, 32, 16, generator=g).to(S.BF16).float()
+    dy = torch.randn(1, 4, 5, 6, 32, generator=g).to(S.BF16)
+    y = S.torch_conv3d(x, w, None, 3, True)
+    y.backward(dy.float())
+    dx = S.torch_conv3d(dy, S.adjoint_weights(w.to(S.BF16)).float(), None, 3, True)
+    torch.testing.assert_close(dx, x.grad, rtol=1e-5, atol=1e-4)
+
+
+def test_targets_round_trip():
+    mask, hs, u_in, _ = gyroid_design(3, nx=48, ny=32, nz=16, buf=4)
+    nx, ny, nz = mask.shape
+    g = torch.Generator().manual_seed(3)
+    rho = 1 + 0.01 * torch.randn(nx, ny, nz, generator=g)
+    u = 0.03 * torch.randn(nx, ny, nz, 3, generator=g)
+    T = 25 + torch.rand(nx, ny, nz, generator=g)
+    solid = torch.from_numpy(mask == 1)
+    rho[solid], u[solid] = 1.0, 0.0
+    tg = S.targets(rho, u, T, u_in, 0.1)
+    assert tg.shape == (1, nz, ny, S.NXP, S.OUT_FIELDS)
+    r2, u2, T2 = S.fields_from_prediction(tg, mask.shape, u_in, 0.1, mask)
+    torch.testing.assert_close(r2, rho, rtol=0, atol=1e-6)
+    torch.testing.assert_close(u2, u, rtol=0, atol=1e-7)
+    torch.testing.assert_close(T2, T, rtol=0, atol=1e-5)
+
+
+def test_features_layout():
+    mask, hs, u_in, _ = gyroid_design(4, nx=48, ny=32, nz=16, buf=4)
+    x = S.features(mask, hs, u_in, device="cpu")
+    assert x.shape == (1, 16, 32, S.NXP, 16) and x.dtype == S.BF16
+    fl = x[0, ..., 0].float()
+    # fluid indicator transposed to [z][y][x]; padding in x is solid (0)
+    assert torch.equal(fl[:, :, :48], torch.from_numpy((mask != 1).transpose(2, 1, 0).astype(np.float32)))
+    assert (fl[:, :, 48:] == 0).all()
+    assert float(x[0, ..., 1].max()) == 1.0
+    assert torch.allclose(x[0, ..., 2].float(), torch.tensor(20 * u_in).to(S.BF16).float())
+    assert (x[0, ..., 3:] == 0).all()

@@ -56,7 +56,7 @@ class ScalarParams(C.Structure):
 class RunOpts(C.Structure):
     _fields_ = [
         ("max_steps", C.c_int), ("stats_every", C.c_int), ("tol_ke", C.c_double), ("tol_T", C.c_double),
-        ("constant_power", C.c_int), ("target_power", C.c_double),
+        ("constant_power", C.c_int), ("target_power", C.c_double), ("min_steps", C.c_int),
     ]
 
 
@@ -106,6 +106,9 @@ SIGNATURES = {
     "xac_lattice_save_state": [_vp, _vp, C.c_size_t, _vp],
     "xac_lattice_load_state": [_vp, _vp, C.c_size_t, _vp],
     "xac_lattice_run": [_vp, C.POINTER(RunOpts), C.POINTER(RunResult), _vp],
+    "xac_conv3d_forward": [_vp, _i, _i, _i, _i, _i, _vp, _vp, _i, _i, _i, _vp, _vp, _vp],
+    "xac_conv3d_weight_grad": [_vp, _i, _i, _i, _i, _i, _vp, _i, _i, _vp, _vp, _vp, _vp],
+    "xac_conv3d_partial_floats": [_i, _i, _i, _i, _i, _i, _i, C.POINTER(C.c_longlong)],
     "xac_batch_create": [C.POINTER(Desc), _i, C.POINTER(_vp), _vp],
     "xac_batch_destroy": [_vp],
     "xac_batch_size": [_vp, C.POINTER(_i)],

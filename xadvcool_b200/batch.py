@@ -84,8 +84,9 @@ class Batch:
         _capi.call("xac_batch_get_tune", self._h, C.byref(b), C.byref(s))
         return int(b.value), int(s.value)
 
-    def run(self, max_steps=30000, stats_every=100, tol_ke=1e-7, tol_T=1e-7) -> list:
-        o = _capi.RunOpts(int(max_steps), int(stats_every), float(tol_ke), float(tol_T), 0, 1.0)
+    def run(self, max_steps=30000, stats_every=100, tol_ke=1e-7, tol_T=1e-7, min_steps=0) -> list:
+        """``min_steps`` > 0 replaces the reference's minimum run length (warm-started designs)."""
+        o = _capi.RunOpts(int(max_steps), int(stats_every), float(tol_ke), float(tol_T), 0, 1.0, int(min_steps))
         res = (_capi.RunResult * self.n)()
         with torch.cuda.device(self.device):
             _capi.call("xac_batch_run", self._h, C.byref(o), res, stream_ptr(self.device))

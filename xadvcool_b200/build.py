@@ -25,6 +25,7 @@ UNITS = [
     ("ops_reference_layout.cu", ["--fmad=false"]),
     ("lattice.cu", ["--fmad=false"]),
     ("stats_noalloc.cu", ["--fmad=false"]),
+    ("conv3d.cu", []),
 ]
 
 

@@ -198,6 +198,15 @@ struct LatticeImpl {
   int red_blocks = 1;
   long long step = 0;
   bool own_pending = true;    // next step reads the initial thermal populations unstreamed
+
+  // src/simulation.py:102-104: no convergence before min(0.6 max_steps, max(5000, 2 nx / u_in)) steps
+  long long reference_min_steps(int max_steps) const {
+    const int a = (int)(0.6 * max_steps);
+    const double mu = u_inlet_nominal > 1e-6 ? u_inlet_nominal : 1e-6;
+    int b = (int)(2.0 * g.nx / mu);
+    if (b < 5000) b = 5000;
+    return a < b ? a : b;
+  }
   long long macro_step = 0;   // rho/u arrays hold the fields of this step
   long long T_step = 0;       // T array holds the field of this step
   cudaStream_t capture = nullptr;
@@ -837,11 +846,7 @@ int xac_lattice_run(xac_lattice* lat, const xac_run_opts* o, xac_run_result* res
   XAC_REQUIRE(o->stats_every > 0 && o->max_steps >= 0, "xac_lattice_run: bad options");
   LatticeImpl& L = lat->impl;
   std::memset(res, 0, sizeof(*res));
-  const int a = (int)(0.6 * o->max_steps);
-  const double mu = L.u_inlet_nominal > 1e-6 ? L.u_inlet_nominal : 1e-6;
-  int b = (int)(2.0 * L.g.nx / mu);
-  if (b < 5000) b = 5000;
-  const long long min_steps = a < b ? a : b;
+  const long long min_steps = o->min_steps > 0 ? o->min_steps : L.reference_min_steps(o->max_steps);
   double prev_ke = 0.0, prev_max_T = 0.0, d_ke = 0.0, dT = 0.0, prev_Q = 0.0, dQ = 1.0;
   double st[kNStats];
   const long long start = L.step;
@@ -1173,11 +1178,7 @@ int xac_batch_run(xac_batch* b, const xac_run_opts* o, xac_run_result* res, void
     d.stat_tiles = (uint32_t)stats_tiles(L.g.ncell);
     d.row_base = row;
     row += d.stat_tiles;
-    const int a = (int)(0.6 * o->max_steps);
-    const double mu = L.u_inlet_nominal > 1e-6 ? L.u_inlet_nominal : 1e-6;
-    int bnd = (int)(2.0 * L.g.nx / mu);
-    if (bnd < 5000) bnd = 5000;
-    d.min_steps = a < bnd ? a : bnd;
+    d.min_steps = o->min_steps > 0 ? o->min_steps : L.reference_min_steps(o->max_steps);
     d.active = 1;
     d.dQ = 1.0;
   }

@@ -150,12 +150,15 @@ class Lattice:
 
     # -- native loop -----------------------------------------------------------------------------
     def run(self, max_steps=40000, stats_every=100, tol_ke=1e-7, tol_T=1e-7, pump_mode="constant_flow",
-            target_power=1.0) -> dict:
-        """src/simulation.py:102-162 in native code; returns steps / convergence diagnostics."""
+            target_power=1.0, min_steps=0) -> dict:
+        """src/simulation.py:102-162 in native code; returns steps / convergence diagnostics.
+
+        ``min_steps`` > 0 replaces the reference's minimum run length before convergence may be declared
+        (min(0.6 max_steps, max(5000, 2 nx / u_in)), src/simulation.py:102-104): warm starts use a short one."""
         if pump_mode not in ("constant_flow", "constant_power"):
             raise ValueError(f"unknown pump_mode {pump_mode!r}")
         o = _capi.RunOpts(int(max_steps), int(stats_every), float(tol_ke), float(tol_T),
-                          1 if pump_mode == "constant_power" else 0, float(target_power))
+                          1 if pump_mode == "constant_power" else 0, float(target_power), int(min_steps))
         r = _capi.RunResult()
         with torch.cuda.device(self.device):
             _capi.call("xac_lattice_run", self._h, C.byref(o), C.byref(r), stream_ptr(self.device))

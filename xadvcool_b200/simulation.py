@@ -26,13 +26,15 @@ def run_simulation(mask,
                    *,
                    precision="fp32",
                    init_fields=None,
-                   keep_lattice=False):
+                   keep_lattice=False,
+                   min_steps=0):
     """src/simulation.py:14-162. Same arguments and the same returned keys
     (u, rho, T as numpy float32 in the reference layout, mask, steps, d_ke, dT_conv, dQ_conv, converged).
 
     Extra keyword-only arguments: ``precision`` ("fp32", "fp16", "bf16" population storage),
     ``init_fields`` = (rho, u, T) CUDA tensors to warm-start from, ``keep_lattice`` to also return the
-    live :class:`Lattice` under key "lattice" (for device-side scalars).
+    live :class:`Lattice` under key "lattice" (for device-side scalars), ``min_steps`` > 0 to replace the
+    reference's minimum run length before convergence (for warm starts).
     """
     nx, ny, nz = np.shape(mask)
     if not silent:
@@ -42,7 +44,7 @@ def run_simulation(mask,
     if init_fields is not None:
         lat.init_fields(*init_fields)
     res = lat.run(max_steps=max_steps, stats_every=stats_every, tol_ke=tol_ke, tol_T=tol_T, pump_mode=pump_mode,
-                  target_power=target_power)
+                  target_power=target_power, min_steps=min_steps)
     if res["diverged"] and not silent:
         st = res["last_stats"]
         max_v, max_T = st[0], st[11]

@@ -1,0 +1,264 @@
+"""Learned warm start end to end: solver-generated training data, surrogate training, and the cold vs warm
+comparison on held-out designs.
+
+    python -m xadvcool_b200.warmstart --train 2000 --heldout 256 --out warmstart.json
+
+Designs are the seeded 148x128x32 gyroid cold plates (designs.gyroid_design); training seeds are 0..n_train-1,
+held-out seeds start at HELDOUT_SEED0 so the two sets are disjoint. Training data are the fields of cold FP32
+solves to the residual tolerance (batched persistent solver), kept resident on the GPU. The comparison times
+each held-out design from mask upload to the scalars (delta_P, R_th), cold-started vs initialised from the
+surrogate's prediction, and reports the relative error of the prediction against the converged fields.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import designs
+from . import surrogate as S
+from .batch import Batch
+from .lattice import Lattice
+
+TAU, POWER, T_IN = 0.55, 0.1, 25.0
+HELDOUT_SEED0 = 1_000_000
+SCALAR_KEYS = ("delta_P", "R_th")
+
+
+def _sync():
+    torch.cuda.synchronize()
+
+
+def design(seed):
+    return designs.gyroid_design(seed)
+
+
+def _spec(mask, hs, u_in):
+    return dict(mask=mask, heat_source=hs, tau_fluid=TAU, heat_power=POWER, t_inlet=T_IN, u_inlet_val=u_in)
+
+
+# ------------------------------------------------------------------------------------------------ data
+def generate(seeds, *, max_steps=30000, tol=1e-6, batch_size=64, log=print):
+    """Cold batched solves of the given seeds -> (features [n,z,y,x,3] bf16, targets [n,z,y,x,5] fp32, info).
+
+    Designs whose cold solve trips the divergence guard (max|u| > 0.17 or T > 1e4, src/simulation.py:146-153;
+    at tau 0.55 most designs with u_in above about 0.045 do so in the impulsive start) give no target and are
+    left out; ``info`` lists every seed with its outcome."""
+    feats, tgts, info = [], [], []
+    for b0 in range(0, len(seeds), batch_size):
+        chunk = seeds[b0:b0 + batch_size]
+        ds = [design(s) for s in chunk]
+        b = Batch([_spec(m, h, u) for m, h, u, _ in ds])
+        res = b.run(max_steps=max_steps, tol_ke=tol, tol_T=tol)
+        for i, (m, h, u, _) in enumerate(ds):
+            info.append({"seed": chunk[i], "u_in": u, "steps": res[i]["steps"], "converged": res[i]["converged"],
+                         "diverged": res[i]["diverged"]})
+            if res[i]["diverged"]:
+                continue
+            rho, uu, T = b.lattice(i).fields()
+            feats.append(S.features(m, h, u)[..., :S.IN_FEATURES].clone())
+            tgts.append(S.targets(rho, uu, T, u, POWER, T_IN))
+        b.close()
+        if log:
+            nconv = sum(r["converged"] for r in res)
+            log(f"generated {b0 + len(chunk)}/{len(seeds)} (batch converged {nconv}/{len(chunk)})")
+    return torch.cat(feats, 0), torch.cat(tgts, 0), info
+
+
+def train_surrogate(feats, tgts, *, epochs=30, batch=4, lr=5e-4, clip=1.0, val_frac=0.05, seed=0, log=print):
+    """Trains the surrogate on resident data (features expanded to 16 channels per mini-batch): AdamW, one-cycle
+    schedule, MSE on per-channel normalised targets, gradient-norm clipping. The last ``val_frac`` of the designs
+    are held back to report a validation loss per epoch."""
+    model = S.Surrogate("cuda", seed=seed)
+    n_all = feats.shape[0]
+    n_val = int(round(val_frac * n_all)) if n_all > 20 else 0
+    n = n_all - n_val
+    mean = tgts[:n].mean(dim=(0, 1, 2, 3))
+    std = tgts[:n].std(dim=(0, 1, 2, 3)).clamp_min(1e-6)
+    model.norm = (mean, std)
+    opt = torch.optim.AdamW(model.parameters(), lr=lr, weight_decay=1e-4)
+    steps = epochs * math.ceil(n / batch)
+    sched = torch.optim.lr_scheduler.OneCycleLR(opt, max_lr=lr, total_steps=steps, pct_start=0.1)
+    g = torch.Generator().manual_seed(seed)
+
+    def inputs(idx):
+        x = torch.zeros((len(idx),) + tuple(feats.shape[1:4]) + (16,), dtype=S.BF16, device="cuda")
+        x[..., :S.IN_FEATURES] = feats[idx]
+        return x
+
+    hist = []
+    for ep in range(epochs):
+        order = torch.randperm(n, generator=g)
+        tot = torch.zeros((), device="cuda")
+        for i in range(0, n, batch):
+            idx = order[i:i + batch].cuda()
+            y = (tgts[idx] - mean) / std
+            loss = torch.nn.functional.mse_loss(model.forward(inputs(idx))[..., :S.OUT_FIELDS], y)
+            opt.zero_grad(set_to_none=True)
+            loss.backward()
+            torch.nn.utils.clip_grad_norm_(model.parameters(), clip)
+            opt.step()
+            sched.step()
+            tot += loss.detach() * len(idx)
+        rec = {"epoch": ep, "mse": float(tot) / n}
+        if n_val:
+            with torch.no_grad():
+                vt = torch.zeros((), device="cuda")
+                for i in range(n, n_all, batch):
+                    idx = torch.arange(i, min(i + batch, n_all), device="cuda")
+                    y = (tgts[idx] - mean) / std
+                    vt += torch.nn.functional.mse_loss(model.forward(inputs(idx))[..., :S.OUT_FIELDS], y,
+                                                       reduction="none").mean(dim=(1, 2, 3, 4)).sum()
+                rec["val_mse"] = float(vt) / n_val
+        hist.append(rec)
+        if log:
+            log(json.dumps(rec))
+    return model, hist
+
+
+# ------------------------------------------------------------------------------------------------ comparison
+def _rel_err(a, b):
+    return float((a - b).norm() / b.norm().clamp_min(1e-30))
+
+
+def solve_solo(mask, hs, u_in, *, model=None, max_steps=150000, tol=1e-6, warm_min_steps=1000):
+    """Mask upload -> (optional surrogate warm start) -> solve -> scalars; returns the record and the lattice."""
+    _sync()
+    t0 = time.perf_counter()
+    lat = Lattice(mask, tau_fluid=TAU, heat_power=POWER, t_inlet=T_IN, u_inlet_val=u_in, heat_source=hs)
+    pred = None
+    if model is not None:
+        pred = S.predict(model, mask, hs, u_in, POWER)
+        lat.init_fields(*pred)
+    r = lat.run(max_steps=max_steps, tol_ke=tol, tol_T=tol, min_steps=warm_min_steps if model is not None else 0)
+    sc = lat.scalars()
+    _sync()
+    rec = {"s": time.perf_counter() - t0, "steps": r["steps"], "converged": r["converged"],
+           "diverged": r["diverged"], **{k: sc[k] for k in SCALAR_KEYS}}
+    return rec, lat, pred
+
+
+def _rel(a, b):
+    return abs(a - b) / abs(b)
+
+
+def compare(model, seeds, *, max_steps=150000, tol=1e-6, warm_min_steps=1000, tight_tol=1e-8, log=print):
+    """Per held-out design: cold and warm solo solves (timed), then, untimed, the cold lattice continued to
+    ``tight_tol`` as the steady-state reference; scalar agreement and the surrogate's field error against it."""
+    rows = []
+    for s in seeds:
+        m, h, u, _ = design(s)
+        cold, lat_c, _ = solve_solo(m, h, u, max_steps=max_steps, tol=tol)
+        warm, lat_w, pred = solve_solo(m, h, u, model=model, max_steps=max_steps, tol=tol,
+                                       warm_min_steps=warm_min_steps)
+        lat_w.close()
+        row = {"seed": s, "u_in": u, "cold": cold, "warm": warm}
+        if not cold["diverged"]:
+            rt = lat_c.run(max_steps=max_steps, tol_ke=tight_tol, tol_T=tight_tol, min_steps=200)
+            sc = lat_c.scalars()
+            tight = {"steps": cold["steps"] + rt["steps"], "converged": rt["converged"],
+                     **{k: sc[k] for k in SCALAR_KEYS}}
+            rho_c, u_c, T_c = lat_c.fields()
+            fluid = torch.from_numpy(np.asarray(m) != 1).cuda()
+            row.update(tight=tight,
+                       dP_rel=_rel(warm["delta_P"], cold["delta_P"]), Rth_rel=_rel(warm["R_th"], cold["R_th"]),
+                       cold_vs_tight={k: _rel(cold[k], tight[k]) for k in SCALAR_KEYS},
+                       warm_vs_tight={k: _rel(warm[k], tight[k]) for k in SCALAR_KEYS},
+                       pred_err={"u": _rel_err(pred[1][fluid], u_c[fluid]),
+                                 "p": _rel_err(pred[0][fluid] - 1, rho_c[fluid] - 1),
+                                 "T": _rel_err(pred[2] - T_IN, T_c - T_IN)},
+                       speedup=cold["s"] / warm["s"])
+        lat_c.close()
+        rows.append(row)
+        if log:
+            log(json.dumps(row))
+    return rows
+
+
+def compare_batched(model, seeds, *, max_steps=150000, tol=1e-6, warm_min_steps=1000):
+    """The held-out designs as one batch, cold vs warm: wall seconds per converged design (mask upload ->
+    scalars of every design), plus the scalar agreement per design."""
+    ds = [design(s) for s in seeds]
+    out = {}
+    for kind in ("cold", "warm"):
+        _sync()
+        t0 = time.perf_counter()
+        b = Batch([_spec(m, h, u) for m, h, u, _ in ds])
+        if kind == "warm":
+            for i, (m, h, u, _) in enumerate(ds):
+                b.lattice(i).init_fields(*S.predict(model, m, h, u, POWER))
+        res = b.run(max_steps=max_steps, tol_ke=tol, tol_T=tol, min_steps=warm_min_steps if kind == "warm" else 0)
+        sc = [b.lattice(i).scalars() for i in range(len(ds))]
+        _sync()
+        wall = time.perf_counter() - t0
+        b.close()
+        nconv = sum(r["converged"] for r in res)
+        out[kind] = {"wall_s": wall, "s_per_design": wall / len(ds), "converged": nconv,
+                     "s_per_converged_design": wall / max(nconv, 1),
+                     "diverged": sum(r["diverged"] for r in res), "steps": [r["steps"] for r in res],
+                     "ok": [bool(r["converged"]) for r in res],
+                     "scalars": [{k: s[k] for k in SCALAR_KEYS} for s in sc]}
+    both = [i for i in range(len(ds)) if out["cold"]["ok"][i] and out["warm"]["ok"][i]]
+    dp = [_rel(out["warm"]["scalars"][i]["delta_P"], out["cold"]["scalars"][i]["delta_P"]) for i in both]
+    rt = [_rel(out["warm"]["scalars"][i]["R_th"], out["cold"]["scalars"][i]["R_th"]) for i in both]
+    out["compared"] = len(both)
+    out["dP_rel_max"] = max(dp) if dp else None
+    out["Rth_rel_max"] = max(rt) if rt else None
+    out["Rth_rel_median"] = float(np.median(rt)) if rt else None
+    out["speedup"] = out["cold"]["s_per_converged_design"] / out["warm"]["s_per_converged_design"]
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--train", type=int, default=2000)
+    ap.add_argument("--heldout", type=int, default=256)
+    ap.add_argument("--solo", type=int, default=16, help="held-out designs also compared one at a time")
+    ap.add_argument("--epochs", type=int, default=30)
+    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--lr", type=float, default=5e-4)
+    ap.add_argument("--gen-max-steps", type=int, default=30000)
+    ap.add_argument("--max-steps", type=int, default=150000)
+    ap.add_argument("--tol", type=float, default=1e-6)
+    ap.add_argument("--warm-min-steps", type=int, default=1000)
+    ap.add_argument("--save", default=None, help="write the trained weights here (torch.save)")
+    ap.add_argument("--load", default=None, help="skip data generation and training; load these weights")
+    ap.add_argument("--out", default="warmstart.json")
+    a = ap.parse_args(argv)
+    report = {"args": vars(a)}
+    if a.load:
+        model = S.Surrogate("cuda")
+        model.load_state_dict(torch.load(a.load))
+    else:
+        t = time.perf_counter()
+        feats, tgts, info = generate(list(range(a.train)), max_steps=a.gen_max_steps, tol=a.tol)
+        report["gen_s"] = time.perf_counter() - t
+        report["gen"] = info
+        report["gen_converged"] = sum(i["converged"] for i in info)
+        report["gen_kept"] = int(feats.shape[0])
+        t = time.perf_counter()
+        model, hist = train_surrogate(feats, tgts, epochs=a.epochs, batch=a.batch, lr=a.lr)
+        _sync()
+        report["train_s"] = time.perf_counter() - t
+        report["train_mse"] = hist
+        del feats, tgts
+        if a.save:
+            torch.save(model.state_dict(), a.save)
+    held = [HELDOUT_SEED0 + i for i in range(a.heldout)]
+    rows = compare(model, held[:a.solo], max_steps=a.max_steps, tol=a.tol, warm_min_steps=a.warm_min_steps)
+    report["solo"] = rows
+    report["batched"] = compare_batched(model, held, max_steps=a.max_steps, tol=a.tol,
+                                        warm_min_steps=a.warm_min_steps)
+    json.dump(report, open(a.out, "w"), indent=1)
+    sp = [r["speedup"] for r in rows if "speedup" in r]
+    print(json.dumps({"solo_speedup_median": float(np.median(sp)) if sp else None,
+                      "batched_speedup": report["batched"]["speedup"],
+                      "dP_rel_max": report["batched"]["dP_rel_max"], "Rth_rel_max": report["batched"]["Rth_rel_max"]}))
+
+
+if __name__ == "__main__":
+    main()
