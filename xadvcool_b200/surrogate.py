@@ -139,6 +139,7 @@ class Surrogate:
         layer("d0b", c0, c0)
         layer("head", c0, OUT_FIELDS, k=1)
         self.norm = None  # per-channel (mean, std) of the targets
+        self.balance = None  # median heat_balance of the training designs
 
     def parameters(self):
         return list(self.params.values())
@@ -190,38 +191,47 @@ class Surrogate:
         sd = {k: v.detach().cpu() for k, v in self.params.items()}
         if self.norm is not None:
             sd["norm.mean"], sd["norm.std"] = (t.cpu() for t in self.norm)
+        if self.balance is not None:
+            sd["balance"] = torch.tensor(self.balance)
         return sd
 
     def load_state_dict(self, sd):
         for k, v in sd.items():
-            if k.startswith("norm."):
+            if k.startswith("norm.") or k == "balance":
                 continue
             self.params[k] = v.to(self.device).requires_grad_(True)
         if "norm.mean" in sd:
             self.norm = (sd["norm.mean"].to(self.device), sd["norm.std"].to(self.device))
+        if "balance" in sd:
+            self.balance = float(sd["balance"])
 
 
 # ------------------------------------------------------------------------------------------------ data
 NXP = 152
 
 
+BC_SOLID, BC_INLET = 1, 2
+OUTLET_PLANE = -2  # x = nx-2, the last plane before the outlet cells (reference layout)
+
+
+def _dev(a, dtype, device):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=dtype)).to(device)
+
+
 def features(mask: np.ndarray, heat_source: np.ndarray | None, u_in: float, device="cuda") -> torch.Tensor:
-    """[1, nz, ny, 152, 16] bf16 input volume from a reference-layout design (x padded with solid)."""
+    """[1, nz, ny, 152, 16] bf16 input volume from a reference-layout design, assembled on the device: fluid
+    indicator, heat map normalised to max 1 (z=0 floor when absent, as src/simulation.py:79-85), 20 u_in; x is
+    padded with solid."""
     nx, ny, nz = mask.shape
-    fl = np.zeros((nz, ny, NXP), np.float32)
-    fl[:, :, :nx] = (np.transpose(mask, (2, 1, 0)) != 1)
-    hs = np.zeros((nz, ny, NXP), np.float32)
+    x = torch.zeros((1, nz, ny, NXP, 16), dtype=BF16, device=device)
+    x[0, :, :, :nx, 0] = (_dev(mask, np.int32, device) != BC_SOLID).permute(2, 1, 0).to(BF16)
     if heat_source is not None:
-        h = np.transpose(np.asarray(heat_source, np.float32), (2, 1, 0))
-        m = h.max()
-        hs[:, :, :nx] = h / m if m > 0 else h
+        h = _dev(heat_source, np.float32, device)
+        x[0, :, :, :nx, 1] = (h / h.max().clamp_min(1e-30)).permute(2, 1, 0).to(BF16)
     else:
-        hs[0, :, :nx] = 1.0
-    x = np.zeros((1, nz, ny, NXP, 16), np.float32)
-    x[0, ..., 0] = fl
-    x[0, ..., 1] = hs
-    x[0, ..., 2] = 20.0 * u_in
-    return torch.from_numpy(x).to(device=device, dtype=BF16)
+        x[0, 0, :, :nx, 1] = 1.0
+    x[..., 2] = 20.0 * u_in
+    return x
 
 
 def targets(rho: torch.Tensor, u: torch.Tensor, T: torch.Tensor, u_in: float, heat_power: float, t_in=25.0):
@@ -234,27 +244,51 @@ def targets(rho: torch.Tensor, u: torch.Tensor, T: torch.Tensor, u_in: float, he
     return out
 
 
+def heat_balance(y: torch.Tensor, x: torch.Tensor, nx: int, u_in) -> torch.Tensor:
+    """Advected heat through the plane x = nx-2 over the injected heat, per design, from scaled fields
+    y [N, z, y, x, >=5] (u/u_in, ..., (T - T_in)/heat_power) and features x (channel 1: heat map):
+    u_in * sum(ux/u_in * dT/P) / sum(heat map). At steady state it is a design-independent constant up to the
+    discretisation (the source adds (1 - omega/2) q per cell and step, thermal_engine3d.py:133-144)."""
+    xo = nx + OUTLET_PLANE
+    u_in = torch.as_tensor(u_in, dtype=torch.float32, device=y.device).reshape(-1)
+    flux = (y[:, :, :, xo, 0] * y[:, :, :, xo, 4]).sum(dim=(1, 2)) * u_in
+    return flux / x[..., 1].float().sum(dim=(1, 2, 3)).clamp_min(1e-30)
+
+
 def fields_from_prediction(pred: torch.Tensor, shape, u_in: float, heat_power: float, mask: np.ndarray,
-                           t_in=25.0):
-    """Prediction [1, nz, ny, 152, >=5] (denormalised scaled targets) -> rho, u, T in the reference layout."""
+                           t_in=25.0, mask_dev: torch.Tensor | None = None):
+    """Prediction [1, nz, ny, 152, >=5] (denormalised scaled targets) -> rho, u, T in the reference layout.
+
+    Solid cells get rho = 1, u = 0. Inlet cells get the cold-start state rho = 1, u = 0, T = t_in
+    (src/simulation.py:63-73): the velocity inlet rebuilds its populations from its own post-collision values
+    only (fluid_engine3d.py:196-224), so its density keeps a memory of its initial value that sets the inflow
+    mass flux for the whole solve. Starting it exactly as a cold start does makes its trajectory, and so the
+    converged delta_P, the cold solve's."""
     nx, ny, nz = shape
     p = pred[0, :, :, :nx, :OUT_FIELDS].permute(2, 1, 0, 3)  # [nx, ny, nz, 5]
     u = (p[..., 0:3] * u_in).contiguous()
     rho = (1.0 + p[..., 3] * u_in).contiguous()
     T = (t_in + p[..., 4] * heat_power).contiguous()
-    solid = torch.from_numpy(np.asarray(mask) == 1).to(pred.device)
-    u[solid] = 0.0
-    rho[solid] = 1.0
+    m = mask_dev if mask_dev is not None else _dev(mask, np.int32, pred.device)
+    solid, inlet = m == BC_SOLID, m == BC_INLET
+    u[solid | inlet] = 0.0
+    rho[solid | inlet] = 1.0
+    T[inlet] = t_in
     return rho.float(), u.float(), T.float()
 
 
-def predict(model: Surrogate, mask, heat_source, u_in, heat_power, device="cuda"):
-    """Warm-start fields for one design (reference layout)."""
+def predict(model: Surrogate, mask, heat_source, u_in, heat_power, device="cuda", balance: float | None = None):
+    """Warm-start fields for one design (reference layout). With ``balance`` (the training designs' median
+    :func:`heat_balance`), the predicted temperature rise is rescaled so the design's advected heat matches its
+    injected heat - the global energy level, which is the slowest mode of the thermal solve."""
     with torch.no_grad():
         x = features(mask, heat_source, u_in, device)
         y = model.forward(x)[..., :OUT_FIELDS]
         mean, std = model.norm
         y = y * std + mean
+        if balance is not None:
+            r = heat_balance(y, x, mask.shape[0], u_in)
+            y[..., 4] *= (balance / r.clamp_min(1e-30)).clamp(0.5, 2.0)
         return fields_from_prediction(y, mask.shape, u_in, heat_power, mask)
 
 
