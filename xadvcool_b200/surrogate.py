@@ -139,7 +139,6 @@ class Surrogate:
         layer("d0b", c0, c0)
         layer("head", c0, OUT_FIELDS, k=1)
         self.norm = None  # per-channel (mean, std) of the targets
-        self.balance = None  # median heat_balance of the training designs
 
     def parameters(self):
         return list(self.params.values())
@@ -191,19 +190,15 @@ class Surrogate:
         sd = {k: v.detach().cpu() for k, v in self.params.items()}
         if self.norm is not None:
             sd["norm.mean"], sd["norm.std"] = (t.cpu() for t in self.norm)
-        if self.balance is not None:
-            sd["balance"] = torch.tensor(self.balance)
         return sd
 
     def load_state_dict(self, sd):
         for k, v in sd.items():
-            if k.startswith("norm.") or k == "balance":
+            if k.startswith("norm."):
                 continue
             self.params[k] = v.to(self.device).requires_grad_(True)
         if "norm.mean" in sd:
             self.norm = (sd["norm.mean"].to(self.device), sd["norm.std"].to(self.device))
-        if "balance" in sd:
-            self.balance = float(sd["balance"])
 
 
 # ------------------------------------------------------------------------------------------------ data
@@ -211,7 +206,6 @@ NXP = 152
 
 
 BC_SOLID, BC_INLET = 1, 2
-OUTLET_PLANE = -2  # x = nx-2, the last plane before the outlet cells (reference layout)
 
 
 def _dev(a, dtype, device):
@@ -244,17 +238,6 @@ def targets(rho: torch.Tensor, u: torch.Tensor, T: torch.Tensor, u_in: float, he
     return out
 
 
-def heat_balance(y: torch.Tensor, x: torch.Tensor, nx: int, u_in) -> torch.Tensor:
-    """Advected heat through the plane x = nx-2 over the injected heat, per design, from scaled fields
-    y [N, z, y, x, >=5] (u/u_in, ..., (T - T_in)/heat_power) and features x (channel 1: heat map):
-    u_in * sum(ux/u_in * dT/P) / sum(heat map). At steady state it is a design-independent constant up to the
-    discretisation (the source adds (1 - omega/2) q per cell and step, thermal_engine3d.py:133-144)."""
-    xo = nx + OUTLET_PLANE
-    u_in = torch.as_tensor(u_in, dtype=torch.float32, device=y.device).reshape(-1)
-    flux = (y[:, :, :, xo, 0] * y[:, :, :, xo, 4]).sum(dim=(1, 2)) * u_in
-    return flux / x[..., 1].float().sum(dim=(1, 2, 3)).clamp_min(1e-30)
-
-
 def fields_from_prediction(pred: torch.Tensor, shape, u_in: float, heat_power: float, mask: np.ndarray,
                            t_in=25.0, mask_dev: torch.Tensor | None = None):
     """Prediction [1, nz, ny, 152, >=5] (denormalised scaled targets) -> rho, u, T in the reference layout.
@@ -277,18 +260,13 @@ def fields_from_prediction(pred: torch.Tensor, shape, u_in: float, heat_power: f
     return rho.float(), u.float(), T.float()
 
 
-def predict(model: Surrogate, mask, heat_source, u_in, heat_power, device="cuda", balance: float | None = None):
-    """Warm-start fields for one design (reference layout). With ``balance`` (the training designs' median
-    :func:`heat_balance`), the predicted temperature rise is rescaled so the design's advected heat matches its
-    injected heat - the global energy level, which is the slowest mode of the thermal solve."""
+def predict(model: Surrogate, mask, heat_source, u_in, heat_power, device="cuda"):
+    """Warm-start fields for one design (reference layout)."""
     with torch.no_grad():
         x = features(mask, heat_source, u_in, device)
         y = model.forward(x)[..., :OUT_FIELDS]
         mean, std = model.norm
         y = y * std + mean
-        if balance is not None:
-            r = heat_balance(y, x, mask.shape[0], u_in)
-            y[..., 4] *= (balance / r.clamp_min(1e-30)).clamp(0.5, 2.0)
         return fields_from_prediction(y, mask.shape, u_in, heat_power, mask)
 
 

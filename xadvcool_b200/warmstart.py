@@ -60,11 +60,8 @@ def generate(seeds, *, max_steps=30000, tol=1e-6, batch_size=64, log=print):
             if res[i]["diverged"]:
                 continue
             rho, uu, T = b.lattice(i).fields()
-            x = S.features(m, h, u)
-            y = S.targets(rho, uu, T, u, POWER, T_IN)
-            info[-1]["heat_balance"] = float(S.heat_balance(y, x, m.shape[0], u))
-            feats.append(x[..., :S.IN_FEATURES].clone())
-            tgts.append(y)
+            feats.append(S.features(m, h, u)[..., :S.IN_FEATURES].clone())
+            tgts.append(S.targets(rho, uu, T, u, POWER, T_IN))
         b.close()
         if log:
             nconv = sum(r["converged"] for r in res)
@@ -124,9 +121,6 @@ def train_surrogate(feats, tgts, *, epochs=30, batch=4, lr=5e-4, clip=1.0, val_f
 
 
 # ------------------------------------------------------------------------------------------------ comparison
-VARIANTS = {"warm": False, "warm_bal": True}  # name -> rescale the temperature rise by the heat balance
-
-
 def _rel_err(a, b):
     return float((a - b).norm() / b.norm().clamp_min(1e-30))
 
@@ -135,7 +129,7 @@ def _rel(a, b):
     return abs(a - b) / abs(b)
 
 
-def solve_solo(mask, hs, u_in, *, model=None, balance=None, max_steps=150000, tol=1e-6, warm_min_steps=1000):
+def solve_solo(mask, hs, u_in, *, model=None, max_steps=150000, tol=1e-6, warm_min_steps=1000):
     """Mask upload -> (optional surrogate warm start) -> solve -> scalars, with the time of each phase; returns
     the record, the lattice and the prediction."""
     _sync()
@@ -145,7 +139,7 @@ def solve_solo(mask, hs, u_in, *, model=None, balance=None, max_steps=150000, to
     t1 = time.perf_counter()
     pred = None
     if model is not None:
-        pred = S.predict(model, mask, hs, u_in, POWER, balance=balance)
+        pred = S.predict(model, mask, hs, u_in, POWER)
         lat.init_fields(*pred)
     _sync()
     t2 = time.perf_counter()
@@ -167,16 +161,10 @@ def compare(model, seeds, *, max_steps=150000, tol=1e-6, warm_min_steps=1000, ti
     for s in seeds:
         m, h, u, _ = design(s)
         cold, lat_c, _ = solve_solo(m, h, u, max_steps=max_steps, tol=tol)
-        row = {"seed": s, "u_in": u, "cold": cold}
-        warm = {}
-        for name, bal in VARIANTS.items():
-            if bal and model.balance is None:
-                continue
-            rec, lat_w, pred = solve_solo(m, h, u, model=model, balance=model.balance if bal else None,
-                                          max_steps=max_steps, tol=tol, warm_min_steps=warm_min_steps)
-            lat_w.close()
-            warm[name] = (rec, pred)
-            row[name] = rec
+        warm, lat_w, pred = solve_solo(m, h, u, model=model, max_steps=max_steps, tol=tol,
+                                       warm_min_steps=warm_min_steps)
+        lat_w.close()
+        row = {"seed": s, "u_in": u, "cold": cold, "warm": warm}
         if not cold["diverged"]:
             rt = lat_c.run(max_steps=max_steps, tol_ke=tight_tol, tol_T=tight_tol, min_steps=200)
             sc = lat_c.scalars()
@@ -184,15 +172,13 @@ def compare(model, seeds, *, max_steps=150000, tol=1e-6, warm_min_steps=1000, ti
                      **{k: sc[k] for k in SCALAR_KEYS}}
             rho_c, u_c, T_c = lat_c.fields()
             fluid = torch.from_numpy(np.asarray(m) != 1).cuda()
-            row.update(tight=tight, cold_vs_tight={k: _rel(cold[k], tight[k]) for k in SCALAR_KEYS})
-            for name, (rec, pred) in warm.items():
-                row[name].update(
-                    vs_cold={k: _rel(rec[k], cold[k]) for k in SCALAR_KEYS},
-                    vs_tight={k: _rel(rec[k], tight[k]) for k in SCALAR_KEYS},
-                    pred_err={"u": _rel_err(pred[1][fluid], u_c[fluid]),
-                              "p": _rel_err(pred[0][fluid] - 1, rho_c[fluid] - 1),
-                              "T": _rel_err(pred[2] - T_IN, T_c - T_IN)},
-                    speedup=cold["s"] / rec["s"])
+            row.update(tight=tight, cold_vs_tight={k: _rel(cold[k], tight[k]) for k in SCALAR_KEYS},
+                       warm_vs_cold={k: _rel(warm[k], cold[k]) for k in SCALAR_KEYS},
+                       warm_vs_tight={k: _rel(warm[k], tight[k]) for k in SCALAR_KEYS},
+                       pred_err={"u": _rel_err(pred[1][fluid], u_c[fluid]),
+                                 "p": _rel_err(pred[0][fluid] - 1, rho_c[fluid] - 1),
+                                 "T": _rel_err(pred[2] - T_IN, T_c - T_IN)},
+                       speedup=cold["s"] / warm["s"])
         lat_c.close()
         rows.append(row)
         if log:
@@ -200,14 +186,14 @@ def compare(model, seeds, *, max_steps=150000, tol=1e-6, warm_min_steps=1000, ti
     return rows
 
 
-def _batched(ds, model, balance, *, max_steps, tol, warm_min_steps):
+def _batched(ds, model, *, max_steps, tol, warm_min_steps):
     """One batch of designs, cold (model None) or warm: wall seconds from mask upload to every design's scalars."""
     _sync()
     t0 = time.perf_counter()
     b = Batch([_spec(m, h, u) for m, h, u, _ in ds])
     if model is not None:
         for i, (m, h, u, _) in enumerate(ds):
-            b.lattice(i).init_fields(*S.predict(model, m, h, u, POWER, balance=balance))
+            b.lattice(i).init_fields(*S.predict(model, m, h, u, POWER))
     res = b.run(max_steps=max_steps, tol_ke=tol, tol_T=tol, min_steps=warm_min_steps if model is not None else 0)
     sc = [b.lattice(i).scalars() for i in range(len(ds))]
     _sync()
@@ -219,41 +205,39 @@ def _batched(ds, model, balance, *, max_steps, tol, warm_min_steps):
             "ok": [bool(r["converged"]) for r in res], "scalars": [{k: s[k] for k in SCALAR_KEYS} for s in sc]}
 
 
-def compare_batched(model, seeds, *, max_steps=150000, tol=1e-6, warm_min_steps=1000):
-    """Batched solves of the held-out designs. The cold batch runs every design; the warm batches run the designs
-    whose cold solve converged (a matched comparison: same designs, same residual), and separately the designs
-    whose cold solve tripped the divergence guard, to count those the warm start solves."""
+def screen(seeds, steps=500):
+    """Seeds whose cold start passes the divergence guard over its first ``steps`` steps (the impulsive start
+    trips it at the first check, step 100, when it trips at all)."""
     ds = [design(s) for s in seeds]
-    out = {"cold": _batched(ds, None, None, max_steps=max_steps, tol=tol, warm_min_steps=warm_min_steps)}
-    ok = [i for i, c in enumerate(out["cold"]["ok"]) if c]
-    bad = [i for i, c in enumerate(out["cold"]["ok"]) if not c]
-    cold_ok_steps = sum(out["cold"]["steps"][i] for i in ok)
-    for name, bal in VARIANTS.items():
-        if bal and model.balance is None:
-            continue
-        w = _batched([ds[i] for i in ok], model, model.balance if bal else None, max_steps=max_steps, tol=tol,
-                     warm_min_steps=warm_min_steps)
-        both = [j for j in range(len(ok)) if w["ok"][j]]
-        dp = [_rel(w["scalars"][j]["delta_P"], out["cold"]["scalars"][ok[j]]["delta_P"]) for j in both]
-        rt = [_rel(w["scalars"][j]["R_th"], out["cold"]["scalars"][ok[j]]["R_th"]) for j in both]
-        w.update(compared=len(both), dP_rel_max=max(dp) if dp else None, Rth_rel_max=max(rt) if rt else None,
-                 dP_rel_median=float(np.median(dp)) if dp else None, Rth_rel_median=float(np.median(rt)) if rt else None,
-                 within_half_percent=sum(1 for a, c in zip(dp, rt) if a <= 5e-3 and c <= 5e-3),
-                 step_ratio=cold_ok_steps / max(sum(w["steps"]), 1),
-                 speedup=(out["cold"]["wall_s"] / len(ds) * len(ok)) / w["wall_s"] if ok else None)
-        out[name] = w
-        if bad:
-            r = _batched([ds[i] for i in bad], model, model.balance if bal else None, max_steps=max_steps, tol=tol,
-                         warm_min_steps=warm_min_steps)
-            out[name + "_cold_failed"] = {k: r[k] for k in ("designs", "converged", "diverged", "steps", "wall_s")}
+    b = Batch([_spec(m, h, u) for m, h, u, _ in ds])
+    res = b.run(max_steps=steps, tol_ke=0.0, tol_T=0.0)
+    b.close()
+    return [s for s, r in zip(seeds, res) if not r["diverged"]], [s for s, r in zip(seeds, res) if r["diverged"]]
+
+
+def compare_batched(model, seeds, *, max_steps=150000, tol=1e-6, warm_min_steps=1000):
+    """Batched solves of the held-out designs whose cold start passes the divergence guard, cold and warm (same
+    designs, same residual): wall seconds per converged design from mask upload to scalars, steps, and the
+    scalar agreement per design. The designs whose cold start trips the guard are then solved warm, to count
+    those the warm start solves."""
+    good, bad = screen(seeds)
+    out = {"screened_out": len(bad)}
+    dg = [design(s) for s in good]
+    out["cold"] = _batched(dg, None, max_steps=max_steps, tol=tol, warm_min_steps=warm_min_steps)
+    out["warm"] = w = _batched(dg, model, max_steps=max_steps, tol=tol, warm_min_steps=warm_min_steps)
+    c = out["cold"]
+    both = [j for j in range(len(dg)) if w["ok"][j] and c["ok"][j]]
+    dp = [_rel(w["scalars"][j]["delta_P"], c["scalars"][j]["delta_P"]) for j in both]
+    rt = [_rel(w["scalars"][j]["R_th"], c["scalars"][j]["R_th"]) for j in both]
+    out.update(compared=len(both), dP_rel_max=max(dp) if dp else None, Rth_rel_max=max(rt) if rt else None,
+               dP_rel_median=float(np.median(dp)) if dp else None, Rth_rel_median=float(np.median(rt)) if rt else None,
+               within_half_percent=sum(1 for a, b in zip(dp, rt) if a <= 5e-3 and b <= 5e-3),
+               step_ratio=sum(c["steps"]) / max(sum(w["steps"]), 1),
+               speedup=c["s_per_converged_design"] / w["s_per_converged_design"])
+    if bad:
+        r = _batched([design(s) for s in bad], model, max_steps=max_steps, tol=tol, warm_min_steps=warm_min_steps)
+        out["warm_cold_tripped"] = {k: r[k] for k in ("designs", "converged", "diverged", "steps", "wall_s")}
     return out
-
-
-def calibrate_balance(info):
-    vals = [i["heat_balance"] for i in info if "heat_balance" in i and i["converged"]]
-    if not vals:
-        vals = [i["heat_balance"] for i in info if "heat_balance" in i]
-    return float(np.median(vals)) if vals else None
 
 
 def main(argv=None):
@@ -271,18 +255,12 @@ def main(argv=None):
     ap.add_argument("--warm-min-steps", type=int, default=1000)
     ap.add_argument("--save", default=None, help="write the trained weights here (torch.save)")
     ap.add_argument("--load", default=None, help="skip data generation and training; load these weights")
-    ap.add_argument("--calib", type=int, default=64,
-                    help="with --load and no stored heat balance: training designs solved to calibrate it")
     ap.add_argument("--out", default="warmstart.json")
     a = ap.parse_args(argv)
     report = {"args": vars(a)}
     if a.load:
         model = S.Surrogate("cuda")
         model.load_state_dict(torch.load(a.load))
-        if model.balance is None and a.calib:
-            _, _, info = generate(list(range(a.calib)), max_steps=a.gen_max_steps, tol=a.tol)
-            model.balance = calibrate_balance(info)
-            report["calib"] = info
     else:
         t = time.perf_counter()
         feats, tgts, info = generate(list(range(a.train)), max_steps=a.gen_max_steps, tol=a.tol)
@@ -290,19 +268,15 @@ def main(argv=None):
         report["gen"] = info
         report["gen_converged"] = sum(i["converged"] for i in info)
         report["gen_kept"] = int(feats.shape[0])
+        print(json.dumps({k: report[k] for k in ("gen_s", "gen_converged", "gen_kept")}), flush=True)
         t = time.perf_counter()
         model, hist = train_surrogate(feats, tgts, epochs=a.epochs, batch=a.batch, lr=a.lr)
         _sync()
         report["train_s"] = time.perf_counter() - t
         report["train_mse"] = hist
-        model.balance = calibrate_balance(info)
         del feats, tgts
         if a.save:
             torch.save(model.state_dict(), a.save)
-    hb = [i["heat_balance"] for i in report.get("gen", report.get("calib", [])) if "heat_balance" in i]
-    if hb:
-        report["heat_balance"] = {"median": float(np.median(hb)), "cv": float(np.std(hb) / abs(np.mean(hb)))}
-        print(json.dumps({"heat_balance": report["heat_balance"]}), flush=True)
     held = [HELDOUT_SEED0 + i for i in range(a.heldout)]
     report["eval"] = {}
     for tol in [float(t) for t in a.eval_tols.split(",")]:
@@ -310,18 +284,16 @@ def main(argv=None):
         bat = compare_batched(model, held, max_steps=a.max_steps, tol=tol, warm_min_steps=a.warm_min_steps)
         report["eval"][f"{tol:g}"] = {"solo": rows, "batched": bat}
         json.dump(report, open(a.out, "w"), indent=1)
-        summ = {"tol": tol, "cold_converged": bat["cold"]["converged"], "designs": len(held)}
-        for name in VARIANTS:
-            if name not in bat:
-                continue
-            sp = [r[name]["speedup"] for r in rows if name in r and "speedup" in r[name]]
-            w = bat[name]
-            summ[name] = {"solo_speedup_median": float(np.median(sp)) if sp else None, "batched_speedup": w["speedup"],
-                          "step_ratio": w["step_ratio"], "compared": w["compared"],
-                          "within_half_percent": w["within_half_percent"], "dP_rel_max": w["dP_rel_max"],
-                          "Rth_rel_max": w["Rth_rel_max"], "Rth_rel_median": w["Rth_rel_median"],
-                          "rescued": bat.get(name + "_cold_failed", {}).get("converged")}
-        print(json.dumps(summ), flush=True)
+        sp = [r["speedup"] for r in rows if "speedup" in r]
+        print(json.dumps({"tol": tol, "designs": len(held), "screened_out": bat["screened_out"],
+                          "solo_speedup_median": float(np.median(sp)) if sp else None,
+                          "batched_speedup": bat["speedup"], "step_ratio": bat["step_ratio"],
+                          "cold_s_per_design": bat["cold"]["s_per_converged_design"],
+                          "warm_s_per_design": bat["warm"]["s_per_converged_design"],
+                          "compared": bat["compared"], "within_half_percent": bat["within_half_percent"],
+                          "dP_rel_max": bat["dP_rel_max"], "Rth_rel_max": bat["Rth_rel_max"],
+                          "Rth_rel_median": bat["Rth_rel_median"],
+                          "rescued": bat.get("warm_cold_tripped", {}).get("converged")}), flush=True)
 
 
 if __name__ == "__main__":
