@@ -204,8 +204,9 @@ int xac_lattice_get_inlet(xac_lattice *lat, double *u_inlet, void *stream);
 int xac_lattice_steps_done(const xac_lattice *lat, long long *steps);
 /* Launch shape of the fused step kernel: threads per block (64, 128, 256) and the visiting order:
  * variant 0 = one thread per cell in memory order; variant 1 = cells grouped by class (bulk fluid, bulk solid,
- * inlet/outlet/y-z-face cells) so that a warp never mixes the fluid and thermal-only work. Results do not depend
- * on it (every cell runs the same arithmetic); xadvcool_b200.autotune picks it. */
+ * inlet/outlet/y-z-face cells) so that a warp never mixes the fluid and thermal-only work; variant 2 = a warp owns
+ * 64 cells and runs the fluid lattice of their non-solid cells in one compacted pass when they are at most 32.
+ * Results do not depend on it (every cell runs the same arithmetic); xadvcool_b200.autotune picks it. */
 int xac_lattice_tune(xac_lattice *lat, int block, int variant);
 int xac_lattice_get_tune(const xac_lattice *lat, int *block, int *variant);
 /* Inputs of generate_dataset.py:80 compute_macroscopic_metrics that are not fields. */
@@ -268,6 +269,9 @@ int xac_conv3d_forward(const void *in, int N, int D, int H, int W, int Ci, const
 int xac_conv3d_weight_grad(const void *in, int N, int D, int H, int W, int Ci, const void *d_out, int Co, int ksize,
                            float *partial, float *dw, float *db, void *stream);
 int xac_conv3d_partial_floats(int N, int D, int H, int W, int Ci, int Co, int ksize, long long *count);
+/* Reads and clears the device-side status of the convolution kernels (synchronises the device): bit 0 set means a
+ * bounded wait inside a tensor-core kernel ran out, and that launch left its output unwritten. */
+int xac_conv3d_status(int *flags);
 
 /* ========================================================================== *
  * Batch: many designs (uneven lattice sizes, one precision) advanced together by ONE persistent cooperative

@@ -19,6 +19,10 @@ SHAPES = [  # N, D, H, W, Ci, Co, ksize
     (1, 3, 5, 7, 32, 48, 3),
     (1, 3, 4, 6, 64, 192, 3),
     (1, 2, 4, 5, 16, 144, 3),
+    (1, 8, 32, 38, 64, 64, 3),     # many 128-voxel tiles, ragged last tile
+    (2, 4, 16, 19, 128, 256, 3),
+    (1, 3, 9, 11, 256, 48, 1),
+    (1, 16, 32, 40, 16, 16, 3),
 ]
 
 
@@ -46,6 +50,7 @@ def test_forward_fp32_out(cuda, shape):
     w = _rand((27 if k == 3 else 1, Co, Ci), g, 0.1).to(S.BF16)
     b = _rand((Co,), g)
     y = S.conv_forward(x, w, b, k, out_fp32=True)
+    assert S.kernel_status() == 0
     ref = _ref_conv(x, w, b, k)
     scale = (x.float().abs().amax() * w.float().abs().sum(dim=(0, 2)).amax()).item()
     # FP32 accumulation of exact BF16 products: only the summation order differs

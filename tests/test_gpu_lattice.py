@@ -201,22 +201,25 @@ def test_16bit_storage_error_vs_fp64_oracle(precision, tol_u, tol_T, cuda):
 @pytest.mark.parametrize("precision", ["fp32", "fp16", "bf16"])
 @pytest.mark.parametrize("block", [64, 128, 256])
 def test_launch_shapes_give_identical_bits(precision, block, cuda):
-    """Memory-order and class-grouped visiting orders at every block size: same bits (and the oracle's)."""
+    """Memory-order, class-grouped and pair-compacted visiting orders at every block size: same bits (and the
+    oracle's). The design has both porous stretches (compacted fluid pass) and all-fluid buffers (two passes)."""
     mask, hs, u_in, _ = designs.gyroid_design(3, nx=48, ny=20, nz=12)
     kw = dict(heat_source=hs, tau_fluid=0.56, u_inlet_val=u_in, heat_power=0.05, precision=precision)
     out = {}
-    for variant in (0, 1):
+    for variant in (0, 1, 2):
         lat = Lattice(mask, **kw)
         lat.tune(block, variant)
         assert lat.get_tune() == (block, variant)
         lat.step(37)
         out[variant] = [t.cpu().numpy() for t in lat.fields()] + [lat.stats()]
         lat.close()
-    for a, b in zip(out[0], out[1]):
-        assert np.array_equal(a, b)
+    for v in (1, 2):
+        for a, b in zip(out[0], out[v]):
+            assert np.array_equal(a, b)
     if precision == "fp32":
         ref = oracle_fields(mask, 37, hs=hs, tau_fluid=0.56, u_inlet_val=u_in, heat_power=0.05)
         assert_exact(ref, *out[1][:3])
+        assert_exact(ref, *out[2][:3])
 
 
 def test_tune_rejects_bad_shapes(cuda):
@@ -224,7 +227,7 @@ def test_tune_rejects_bad_shapes(cuda):
     with pytest.raises(Exception):
         lat.tune(96, 0)
     with pytest.raises(Exception):
-        lat.tune(128, 2)
+        lat.tune(128, 3)
 
 
 def test_autotune_picks_a_valid_shape_without_touching_results(cuda, tmp_path, monkeypatch):

@@ -109,6 +109,7 @@ SIGNATURES = {
     "xac_conv3d_forward": [_vp, _i, _i, _i, _i, _i, _vp, _vp, _i, _i, _i, _vp, _vp, _vp],
     "xac_conv3d_weight_grad": [_vp, _i, _i, _i, _i, _i, _vp, _i, _i, _vp, _vp, _vp, _vp],
     "xac_conv3d_partial_floats": [_i, _i, _i, _i, _i, _i, _i, C.POINTER(C.c_longlong)],
+    "xac_conv3d_status": [C.POINTER(_i)],
     "xac_batch_create": [C.POINTER(Desc), _i, C.POINTER(_vp), _vp],
     "xac_batch_destroy": [_vp],
     "xac_batch_size": [_vp, C.POINTER(_i)],

@@ -15,7 +15,7 @@ import numpy as np
 import torch
 
 BLOCKS = (64, 128, 256)
-VARIANTS = (0, 1)  # 0: memory order, 1: grouped by cell class
+VARIANTS = (0, 1, 2)  # 0: memory order, 1: grouped by cell class, 2: pair-compacted fluid pass
 
 
 def _cache_path() -> Path:

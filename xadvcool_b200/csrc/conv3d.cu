@@ -130,6 +130,236 @@ __global__ void __launch_bounds__(128) conv_fwd_kernel(const __nv_bfloat16* __re
   }
 }
 
+// ---- forward / data grad on the 5th-generation tensor cores (tcgen05) ------------------------------------
+// One CTA of 128 threads computes a 128-voxel x Co tile: D[128][Co] (FP32, in tensor memory) =
+// sum over K = taps x Ci of A[voxel][k] * B[co][k]. K is walked in stages of one tap x BK channels:
+//   * all 128 threads gather the stage's operands into shared memory with 16-byte cp.async copies (zero-filled
+//     where the neighbour is outside the volume), A row r = voxel m0 + r, B row n = output channel n;
+//   * one thread issues the stage's BK/16 tcgen05.mma (kind::f16, BF16 in, FP32 accumulate) and a
+//     tcgen05.commit that frees the stage when those MMAs have read it;
+//   * a ring of kStages stages overlaps the gathers with the MMAs (mbarriers "full" and "empty").
+// Shared-memory operand layout (K-major, no swizzle): 16-byte chunks of 8 channels, [BK/8][rows][8], so a core
+// matrix (8 rows x 16 bytes) is 128 contiguous bytes, 8-row groups are 128 bytes apart (stride byte offset) and
+// the two 8-channel halves of one K = 16 MMA step are rows*16 bytes apart (leading byte offset).
+// Epilogue: warp w reads tensor-memory lanes 32w..32w+31 (its voxels) 16 columns at a time, adds the bias,
+// applies GELU if asked, and stores BF16 or FP32.
+// Every wait is bounded: a wait that runs out sets g_conv_status, the CTA stops issuing work, waits (bounded) for
+// the MMAs it issued, frees its tensor memory and returns.
+constexpr int kTcM = 128;
+constexpr int kTcStages = 4;
+constexpr uint32_t kTcSpin = 1u << 22;
+__device__ unsigned int g_conv_status;  // bit 0: a wait ran out
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (uint32_t i = 0; i < kTcSpin; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  atomicOr(&g_conv_status, 1u);
+  return false;
+}
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// shared-memory matrix descriptor: K-major, no swizzle (layout type 0), descriptor version 1
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// instruction descriptor, kind::f16: FP32 accumulator, BF16 A and B, both K-major, N = n, M = 128
+__host__ __device__ constexpr uint32_t tc_idesc(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
+}
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+struct TcConv {
+  int BK;          // channels per stage (16..64, divides Ci)
+  int kt;          // stages of K: taps * Ci / BK
+  uint32_t ncols;  // tensor-memory columns allocated (power of two >= max(32, Co))
+};
+
+__global__ void __launch_bounds__(128, 1) conv_fwd_tc_kernel(const __nv_bfloat16* __restrict__ in,
+                                                             const __nv_bfloat16* __restrict__ w,
+                                                             const float* __restrict__ bias, ConvShape s, int act,
+                                                             TcConv t, __nv_bfloat16* __restrict__ out_bf16,
+                                                             float* __restrict__ out_f32) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bars[2 * kTcStages + 1];  // full[s], empty[s], done
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int Co = s.Co, BK = t.BK, chunks = BK >> 3;
+  const long long V = (long long)s.N * s.D * s.H * s.W;
+  const long long m0 = (long long)blockIdx.x * kTcM;
+  const uint32_t a_bytes = kTcM * BK * 2, b_bytes = (uint32_t)Co * BK * 2, stage_bytes = a_bytes + b_bytes;
+  const uint32_t sbase = smem_addr(smem);
+  const uint32_t bar0 = smem_addr(bars);
+  auto full = [&](int st) { return bar0 + 8u * st; };
+  auto empty = [&](int st) { return bar0 + 8u * (kTcStages + st); };
+  const uint32_t done_bar = bar0 + 8u * (2 * kTcStages);
+
+  if (tid == 0) {
+    for (int st = 0; st < kTcStages; ++st) {
+      mbar_init(full(st), 128);
+      mbar_init(empty(st), 1);
+    }
+    mbar_init(done_bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
+                 "r"(t.ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+
+  // this thread's A row: voxel m0 + tid
+  const long long v = m0 + tid;
+  const bool vrow = v < V;
+  const VoxelCoord vc = decode(vrow ? v : 0, s);
+  const int ci_chunks = s.Ci / BK;
+  const uint32_t idesc = tc_idesc(Co);
+
+  auto load_stage = [&](int k, int st) {
+    const int tap = k / ci_chunks, kc = k - tap * ci_chunks;
+    const int dz = s.ksize == 3 ? tap / 9 - 1 : 0, dy = s.ksize == 3 ? (tap / 3) % 3 - 1 : 0,
+              dx = s.ksize == 3 ? tap % 3 - 1 : 0;
+    const long long nb = vrow ? neighbour(vc, dz, dy, dx, s) : -1;
+    const uint32_t a_st = sbase + (uint32_t)st * stage_bytes, b_st = a_st + a_bytes;
+    const __nv_bfloat16* asrc = nb >= 0 ? in + nb * s.Ci + kc * BK : in;
+    for (int j = 0; j < chunks; ++j)
+      cp_async16(a_st + (uint32_t)(j * kTcM + tid) * 16u, asrc + (nb >= 0 ? j * 8 : 0), nb >= 0 ? 16u : 0u);
+    const __nv_bfloat16* wt = w + ((long long)tap * Co) * s.Ci + kc * BK;
+    for (int e = tid; e < Co * chunks; e += 128) {
+      const int n = e / chunks, j = e - n * chunks;
+      cp_async16(b_st + (uint32_t)(j * Co + n) * 16u, wt + (long long)n * s.Ci + j * 8, 16u);
+    }
+  };
+  auto mma_stage = [&](int k, int st) {
+    const uint32_t a_st = sbase + (uint32_t)st * stage_bytes, b_st = a_st + a_bytes;
+    for (int q = 0; q < BK / 16; ++q) {
+      const uint64_t ad = smem_desc(a_st + (uint32_t)(2 * q) * kTcM * 16u, kTcM * 16u, 128u);
+      const uint64_t bd = smem_desc(b_st + (uint32_t)(2 * q) * Co * 16u, (uint32_t)Co * 16u, 128u);
+      tc_mma(tmem, ad, bd, idesc, (k > 0 || q > 0) ? 1u : 0u);
+    }
+    tc_commit(empty(st));
+  };
+
+  const int KT = t.kt;
+  for (int k = 0; k < KT + kTcStages - 1; ++k) {
+    if (k < KT) {
+      const int st = k % kTcStages;
+      if (k >= kTcStages && !mbar_wait(empty(st), ((k / kTcStages) - 1) & 1)) abort_flag = 1;
+      if (abort_flag) break;
+      load_stage(k, st);
+    }
+    cp_async_commit();
+    const int kc = k - (kTcStages - 1);  // the stage whose copies this thread now completes
+    if (kc >= 0) {
+      cp_async_wait<kTcStages - 1>();
+      fence_proxy_async();
+      mbar_arrive(full(kc % kTcStages));
+      if (warp == 0) {  // the whole warp waits, lane 0 issues
+        if (mbar_wait(full(kc % kTcStages), (kc / kTcStages) & 1)) {
+          tc_fence_after();
+          if (lane == 0) mma_stage(kc, kc % kTcStages);
+        } else {
+          abort_flag = 1;
+        }
+        __syncwarp();
+      }
+    }
+    if (abort_flag) break;
+  }
+  cp_async_wait<0>();
+  // the last commit (or, after an abort, a fresh one) arrives on done_bar when every issued MMA has finished
+  if (tid == 0) tc_commit(done_bar);
+  const int drained = mbar_wait(done_bar, 0) ? 1 : 0;
+  const bool ok = __syncthreads_and(drained) && !abort_flag;  // uniform: every thread has left the loop
+  tc_fence_after();
+  if (ok) {
+    const long long vr = m0 + warp * 32 + lane;
+    for (int c0 = 0; c0 < Co; c0 += 16) {
+      float x[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, x);
+      if (vr < V) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          float y = x[i] + (bias ? __ldg(bias + c0 + i) : 0.0f);
+          x[i] = act == 1 ? gelu(y) : y;
+        }
+        if (out_bf16) {
+          uint4 pk[2];
+          uint32_t* pw = reinterpret_cast<uint32_t*>(pk);
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            __nv_bfloat162 b2 = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
+            pw[i] = *reinterpret_cast<uint32_t*>(&b2);
+          }
+          uint4* dst = reinterpret_cast<uint4*>(out_bf16 + vr * Co + c0);
+          dst[0] = pk[0];
+          dst[1] = pk[1];
+        } else {
+          float4* dst = reinterpret_cast<float4*>(out_f32 + vr * Co + c0);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) dst[i] = make_float4(x[4 * i], x[4 * i + 1], x[4 * i + 2], x[4 * i + 3]);
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(t.ncols));
+  }
+}
+
 // ---- weight grad ------------------------------------------------------------------------------------
 // Block: one tap, one 16 (co) x 16 (ci) tile, one chunk of voxels (the GEMM's K). 4 warps split the chunk's k16
 // steps; their partials are added in warp order through shared memory. Output: partial[chunk][tap][co][ci].
@@ -256,21 +486,23 @@ int xac_conv3d_forward(const void* in, int N, int D, int H, int W, int Ci, const
               "xac_conv3d_forward: give exactly one output");
   XAC_REQUIRE(activation == 0 || activation == 1, "xac_conv3d_forward: activation must be 0 (none) or 1 (GELU)");
   const long long V = (long long)N * D * H * W;
-  // output channels per block: the widest multiple of 16 up to 128 that divides Co
-  int slice = 128;
-  while (Co % slice != 0) slice -= 16;
-  const dim3 grid((unsigned)((V + 63) / 64), (unsigned)(Co / slice));
-  cudaStream_t st = as_stream(stream);
-  const auto* x = (const __nv_bfloat16*)in;
-  const auto* wt = (const __nv_bfloat16*)weight;
-  auto* ob = (__nv_bfloat16*)out_bf16;
-  switch (slice / 8) {
-#define XAC_CO(NT) \
-  case NT: conv_fwd_kernel<NT><<<grid, 128, 0, st>>>(x, wt, bias, s, activation, ob, out_f32); break;
-    XAC_CO(2) XAC_CO(4) XAC_CO(6) XAC_CO(8) XAC_CO(10) XAC_CO(12) XAC_CO(14) XAC_CO(16)
-#undef XAC_CO
-    default: set_error("xac_conv3d_forward: unsupported channel slice %d", slice); return XAC_EINVAL;
+  TcConv t;
+  t.BK = 64;
+  while (Ci % t.BK != 0) t.BK -= 16;  // 64, 48, 32 or 16
+  t.kt = (ksize == 3 ? 27 : 1) * (Ci / t.BK);
+  t.ncols = 32;
+  while ((int)t.ncols < Co) t.ncols <<= 1;
+  const size_t smem = (size_t)kTcStages * (kTcM + Co) * t.BK * 2;
+  static bool attr_set = false;  // the attribute is per device function; set once per process
+  if (!attr_set) {
+    XAC_CUDA(cudaFuncSetAttribute(conv_fwd_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)((size_t)kTcStages * (kTcM + 256) * 64 * 2)));
+    attr_set = true;
   }
+  const unsigned grid = (unsigned)((V + kTcM - 1) / kTcM);
+  conv_fwd_tc_kernel<<<grid, 128, smem, as_stream(stream)>>>((const __nv_bfloat16*)in,
+                                                             (const __nv_bfloat16*)weight, bias, s, activation, t,
+                                                             (__nv_bfloat16*)out_bf16, out_f32);
   XAC_CUDA(cudaGetLastError());
   return XAC_OK;
 }
@@ -296,6 +528,15 @@ int xac_conv3d_weight_grad(const void* in, int N, int D, int H, int W, int Ci, c
     bias_grad_final_kernel<<<1, Co, 0, st>>>(partial, kBiasBlocks, Co, db);
   }
   XAC_CUDA(cudaGetLastError());
+  return XAC_OK;
+}
+
+int xac_conv3d_status(int* flags) {
+  XAC_REQUIRE(flags, "xac_conv3d_status: null pointer");
+  unsigned int v = 0, zero = 0;
+  XAC_CUDA(cudaMemcpyFromSymbol(&v, g_conv_status, sizeof(v)));
+  XAC_CUDA(cudaMemcpyToSymbol(g_conv_status, &zero, sizeof(zero)));
+  *flags = (int)v;
   return XAC_OK;
 }
 

@@ -180,7 +180,7 @@ struct LatticeImpl {
   float relax[5] = {1.0f, 1.0f, 1.0f, 0.5f, 0.5f};  // omega_f, omega_tf, omega_ts, srcf_f, srcf_s (device-computed)
   float u_in_host = 0.0f;
   int tune_block = 128;  // threads per block of the step kernel
-  int tune_variant = 0;  // 0: cells in memory order; 1: cells grouped by class (bulk fluid / bulk solid / other)
+  int tune_variant = 0;  // 0: cells in memory order; 1: cells grouped by class; 2: pair-compacted fluid pass
   uint32_t* cells = nullptr;                 // class-grouped cell list (kNoCell padding)
   uint32_t cells_len = 0, end_fluid = 0, end_solid = 0;
 
@@ -268,6 +268,15 @@ struct LatticeImpl {
 #define XAC_LAUNCH(M, O)                                                                                   \
   coupled_step_grouped_kernel<S, M, O><<<grid, b, 0, s>>>(cells, end_fluid, end_solid, Pin, Pout, Qin, Qout, \
                                                           link, qsrc, u_in, rho, ux, uy, uz, T, p)
+      if (macro && own) XAC_LAUNCH(true, true);
+      else if (macro) XAC_LAUNCH(true, false);
+      else if (own) XAC_LAUNCH(false, true);
+      else XAC_LAUNCH(false, false);
+#undef XAC_LAUNCH
+    } else if (tune_variant == 2) {
+      const unsigned grid = grid_for(g.ncell, 2 * b);  // 64 cells per warp
+#define XAC_LAUNCH(M, O) \
+  coupled_pair_kernel<S, M, O><<<grid, b, 0, s>>>(Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux, uy, uz, T, p)
       if (macro && own) XAC_LAUNCH(true, true);
       else if (macro) XAC_LAUNCH(true, false);
       else if (own) XAC_LAUNCH(false, true);
@@ -729,7 +738,7 @@ int xac_lattice_tune(xac_lattice* lat, int block, int variant) {
   XAC_REQUIRE(lat, "xac_lattice_tune: null lattice");
   XAC_REQUIRE(block == 64 || block == 128 || block == 256, "xac_lattice_tune: block must be 64, 128 or 256 (got %d)",
               block);
-  XAC_REQUIRE(variant == 0 || variant == 1, "xac_lattice_tune: variant must be 0 or 1 (got %d)", variant);
+  XAC_REQUIRE(variant >= 0 && variant <= 2, "xac_lattice_tune: variant must be 0, 1 or 2 (got %d)", variant);
   LatticeImpl& L = lat->impl;
   std::lock_guard<std::mutex> g(L.mu);
   if (L.tune_block != block || L.tune_variant != variant) {

@@ -98,8 +98,7 @@ struct StepParams {
   // kernels, hoisted out of the per-cell work): fluid omega, thermal omega fluid/solid, source factor fluid/solid
   float omega_f, omega_tf, omega_ts, srcf_f, srcf_s;
   // element offsets: plane[i] = i*N; pull[i] = i*N - (ex + ey*nx + ez*nx*ny), so that the source of direction i
-  // for cell c is pop[c + pull[i]] and its own value is pop[c + plane[i]]. Kernels form one 64-bit pointer per
-  // cell and add these warp-uniform offsets, which the hardware folds into the load/store address.
+  // for cell c is pop[c + pull[i]] and its own value is pop[c + plane[i]] (32-bit indices: all are below 19 N).
   int32_t plane[kQ];
   int32_t pull[kQ];
 };
@@ -112,142 +111,148 @@ __device__ __forceinline__ unsigned sector_group(int lane) {
   return sizeof(S) == 4 ? (0xFFu << (lane & ~7)) : (0xFFFFu << (lane & ~15));
 }
 
-// One coupled step for one cell per thread (see the scheme at the top of this file). Solid cells carry no
+// The three parts of one coupled step of cell c (see the scheme at the top of this file). Solid cells carry no
 // fluid work: their fluid populations are the rest equilibrium w_i for ever (fluid_engine3d.py:193-194 never
 // streams them, and they start at rho=1, u=0); a solid lane still stores w_i when a fluid lane shares its
 // sector, so every sector of the fluid output is written whole.
-template <typename S, bool kMacro, bool kOwn, bool kCoherent = false>
-__device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restrict__ Pin, S* __restrict__ Pout,
-                                             const S* __restrict__ Qin, S* __restrict__ Qout,
-                                             const uint32_t* __restrict__ link, const float* __restrict__ qsrc,
-                                             const float* __restrict__ u_in_ptr, float* __restrict__ rho_o,
-                                             float* __restrict__ ux_o, float* __restrict__ uy_o,
-                                             float* __restrict__ uz_o, const float* __restrict__ T0,
-                                             const StepParams& p, const bool valid, const uint32_t lw,
-                                             const bool fill_solid) {
+// Population (direction i, cell c) is element c + plane[i] of its array; a pulled source is c + pull[i]. Both
+// indices are formed in 32 bits (every one is non-negative and below 19 N) so each access costs one integer add
+// and one widening multiply-add off the array base.
+
+// fluid lattice of a non-solid cell: pull with the boundary rules, moments, BGK collision; returns u
+template <typename S, bool kMacro, bool kCoherent = false>
+__device__ __forceinline__ void fluid_cell(const uint32_t c, const S* __restrict__ Pin, S* __restrict__ Pout,
+                                           const float* __restrict__ u_in_ptr, float* __restrict__ rho_o,
+                                           float* __restrict__ ux_o, float* __restrict__ uy_o,
+                                           float* __restrict__ uz_o, const StepParams& p, const uint32_t lw,
+                                           float& ux, float& uy, float& uz) {
   const int type = link_type(lw);
-  const bool fluid = valid && type != kSolid;
-  const S* __restrict__ Pc = Pin + c;  // this cell's element in plane 0
-  const S* __restrict__ Qc = Qin + c;
-  S* __restrict__ Po = Pout + c;
-  S* __restrict__ Qo = Qout + c;
-
-  float ux = 0.0f, uy = 0.0f, uz = 0.0f;
-
-  // ------------------------------------------------------------------ fluid lattice
-  if (fluid) {
-    float F[kQ];
-    if (type == kInlet) {
-      // src/fluid_engine3d.py:197-244: no pull; unknown populations from the known ones
-      float k[kQ];
-#define XAC_LD_OWN(I) k[I] = Pop<S>::template ld<kCoherent>(Pc + p.plane[I], w_of(I));
-      XAC_FOR19(XAC_LD_OWN)
+  const S* __restrict__ Pc = Pin + c;  // outlet cells copy from Pc - 1
+  float F[kQ];
+  if (type == kInlet) {
+    // src/fluid_engine3d.py:197-244: no pull; unknown populations from the known ones
+    float k[kQ];
+#define XAC_LD_OWN(I) k[I] = Pop<S>::template ld<kCoherent>(Pin + (c + p.plane[I]), w_of(I));
+    XAC_FOR19(XAC_LD_OWN)
 #undef XAC_LD_OWN
-      const float ux_in = __ldg(u_in_ptr);
-      const float rn = (((((((((k[0] + k[3]) + k[4]) + k[5]) + k[6]) + k[15]) + k[16]) + k[17]) + k[18]) +
-                        2.0f * ((((k[2] + k[8]) + k[10]) + k[12]) + k[14])) /
-                       (1.0f - ux_in);
-      const float c23 = 2.0f / 3.0f, c16 = 1.0f / 6.0f;
-      F[0] = k[0];
-      F[1] = k[2] + (c23 * rn) * ux_in;
-      F[2] = k[2];
-      F[3] = k[3];
-      F[4] = k[4];
-      F[5] = k[5];
-      F[6] = k[6];
-      F[7] = k[10] + (c16 * rn) * ux_in;
-      F[8] = k[8];
-      F[9] = k[8] + (c16 * rn) * ux_in;
-      F[10] = k[10];
-      F[11] = k[14] + (c16 * rn) * ux_in;
-      F[12] = k[12];
-      F[13] = k[12] + (c16 * rn) * ux_in;
-      F[14] = k[14];
-      F[15] = k[15];
-      F[16] = k[16];
-      F[17] = k[17];
-      F[18] = k[18];
-    } else if (type == kOutlet) {
-      // src/fluid_engine3d.py:247-259: copy post-collision (x-1) and rescale to rho_outlet
-      const S* __restrict__ Ps = (lw & kXLoBit) ? Pc : Pc - 1;
-      float sum = 0.0f;
+    const float ux_in = __ldg(u_in_ptr);
+    const float rn = (((((((((k[0] + k[3]) + k[4]) + k[5]) + k[6]) + k[15]) + k[16]) + k[17]) + k[18]) +
+                      2.0f * ((((k[2] + k[8]) + k[10]) + k[12]) + k[14])) /
+                     (1.0f - ux_in);
+    const float c23 = 2.0f / 3.0f, c16 = 1.0f / 6.0f;
+    F[0] = k[0];
+    F[1] = k[2] + (c23 * rn) * ux_in;
+    F[2] = k[2];
+    F[3] = k[3];
+    F[4] = k[4];
+    F[5] = k[5];
+    F[6] = k[6];
+    F[7] = k[10] + (c16 * rn) * ux_in;
+    F[8] = k[8];
+    F[9] = k[8] + (c16 * rn) * ux_in;
+    F[10] = k[10];
+    F[11] = k[14] + (c16 * rn) * ux_in;
+    F[12] = k[12];
+    F[13] = k[12] + (c16 * rn) * ux_in;
+    F[14] = k[14];
+    F[15] = k[15];
+    F[16] = k[16];
+    F[17] = k[17];
+    F[18] = k[18];
+  } else if (type == kOutlet) {
+    // src/fluid_engine3d.py:247-259: copy post-collision (x-1) and rescale to rho_outlet
+    const S* __restrict__ Ps = (lw & kXLoBit) ? Pc : Pc - 1;
+    float sum = 0.0f;
 #define XAC_LD_OUT(I)                              \
-  F[I] = Pop<S>::template ld<kCoherent>(Ps + p.plane[I], w_of(I));     \
-  sum += F[I];
-      XAC_FOR19(XAC_LD_OUT)
+F[I] = Pop<S>::template ld<kCoherent>(Ps + p.plane[I], w_of(I));     \
+sum += F[I];
+    XAC_FOR19(XAC_LD_OUT)
 #undef XAC_LD_OUT
-      if (sum > 1e-6f) {
-        const float sc = p.rho_out / sum;
+    if (sum > 1e-6f) {
+      const float sc = p.rho_out / sum;
 #pragma unroll
-        for (int i = 0; i < kQ; ++i) F[i] *= sc;
-      }
-    } else {
-      // src/fluid_engine3d.py:262-272: pull, halfway bounce-back on out-of-domain or solid sources
-#define XAC_LD_PULL(I)                                                                                      \
-  F[I] = ((lw >> I) & 1u) ? Pop<S>::template ld<kCoherent>(Pc + p.plane[opp_of(I)], w_of(I)) : Pop<S>::template ld<kCoherent>(Pc + p.pull[I], w_of(I));
-      XAC_FOR19(XAC_LD_PULL)
-#undef XAC_LD_PULL
+      for (int i = 0; i < kQ; ++i) F[i] *= sc;
     }
-    // src/fluid_engine3d.py:85-113 moments, reference summation order
+  } else {
+    // src/fluid_engine3d.py:262-272: pull, halfway bounce-back on out-of-domain or solid sources
+#define XAC_LD_PULL(I)                                                                                      \
+F[I] = ((lw >> I) & 1u) ? Pop<S>::template ld<kCoherent>(Pin + (c + p.plane[opp_of(I)]), w_of(I)) : Pop<S>::template ld<kCoherent>(Pin + (c + p.pull[I]), w_of(I));
+    XAC_FOR19(XAC_LD_PULL)
+#undef XAC_LD_PULL
+  }
+  // src/fluid_engine3d.py:85-113 moments, reference summation order
+  float r = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f;
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    r += F[i];
+    if (ex_of(i) != 0) mx += ex_of(i) > 0 ? F[i] : -F[i];
+    if (ey_of(i) != 0) my += ey_of(i) > 0 ? F[i] : -F[i];
+    if (ez_of(i) != 0) mz += ez_of(i) > 0 ? F[i] : -F[i];
+  }
+  if (r > 1e-10f) {
+    ux = mx / r;
+    uy = my / r;
+    uz = mz / r;
+  }
+  if (kMacro) {
+    rho_o[c] = r;
+    ux_o[c] = ux;
+    uy_o[c] = uy;
+    uz_o[c] = uz;
+  }
+  // src/fluid_engine3d.py:157-173 BGK with the equilibrium in registers
+  const float omega = p.omega_f;
+  const float usq15 = 1.5f * ((ux * ux + uy * uy) + uz * uz);
+#define XAC_COLLIDE(I)                                                            \
+{                                                                               \
+  const float fe = feq_term(w_of(I) * r, edotu<I>(ux, uy, uz), usq15);         \
+  Pop<S>::st(Pout + (c + p.plane[I]), F[I] - omega * (F[I] - fe), w_of(I));             \
+}
+  XAC_FOR19(XAC_COLLIDE)
+#undef XAC_COLLIDE
+}
+
+// fluid lattice of a solid cell: moments of the frozen populations on macro steps, w_i fill of shared sectors
+template <typename S, bool kMacro, bool kCoherent = false>
+__device__ __forceinline__ void solid_cell(const uint32_t c, const S* __restrict__ Pin, S* __restrict__ Pout,
+                                           float* __restrict__ rho_o, float* __restrict__ ux_o,
+                                           float* __restrict__ uy_o, float* __restrict__ uz_o,
+                                           const StepParams& p, const bool fill_solid) {
+  if (kMacro) {
+    // moments of the frozen solid populations, as the reference's macroscopic kernel computes them
     float r = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f;
 #pragma unroll
     for (int i = 0; i < kQ; ++i) {
-      r += F[i];
-      if (ex_of(i) != 0) mx += ex_of(i) > 0 ? F[i] : -F[i];
-      if (ey_of(i) != 0) my += ey_of(i) > 0 ? F[i] : -F[i];
-      if (ez_of(i) != 0) mz += ez_of(i) > 0 ? F[i] : -F[i];
+      const float v = Pop<S>::template ld<kCoherent>(Pin + (c + p.plane[i]), w_of(i));
+      r += v;
+      if (ex_of(i) != 0) mx += ex_of(i) > 0 ? v : -v;
+      if (ey_of(i) != 0) my += ey_of(i) > 0 ? v : -v;
+      if (ez_of(i) != 0) mz += ez_of(i) > 0 ? v : -v;
     }
-    if (r > 1e-10f) {
-      ux = mx / r;
-      uy = my / r;
-      uz = mz / r;
-    }
-    if (kMacro) {
-      rho_o[c] = r;
-      ux_o[c] = ux;
-      uy_o[c] = uy;
-      uz_o[c] = uz;
-    }
-    // src/fluid_engine3d.py:157-173 BGK with the equilibrium in registers
-    const float omega = p.omega_f;
-    const float usq15 = 1.5f * ((ux * ux + uy * uy) + uz * uz);
-#define XAC_COLLIDE(I)                                                            \
-  {                                                                               \
-    const float fe = feq_term(w_of(I) * r, edotu<I>(ux, uy, uz), usq15);         \
-    Pop<S>::st(Po + p.plane[I], F[I] - omega * (F[I] - fe), w_of(I));             \
+    rho_o[c] = r;
+    ux_o[c] = r > 1e-10f ? mx / r : 0.0f;
+    uy_o[c] = r > 1e-10f ? my / r : 0.0f;
+    uz_o[c] = r > 1e-10f ? mz / r : 0.0f;
   }
-    XAC_FOR19(XAC_COLLIDE)
-#undef XAC_COLLIDE
-  } else if (valid) {
-    if (kMacro) {
-      // moments of the frozen solid populations, as the reference's macroscopic kernel computes them
-      float r = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f;
+  if (fill_solid) {
 #pragma unroll
-      for (int i = 0; i < kQ; ++i) {
-        const float v = Pop<S>::template ld<kCoherent>(Pc + p.plane[i], w_of(i));
-        r += v;
-        if (ex_of(i) != 0) mx += ex_of(i) > 0 ? v : -v;
-        if (ey_of(i) != 0) my += ey_of(i) > 0 ? v : -v;
-        if (ez_of(i) != 0) mz += ez_of(i) > 0 ? v : -v;
-      }
-      rho_o[c] = r;
-      ux_o[c] = r > 1e-10f ? mx / r : 0.0f;
-      uy_o[c] = r > 1e-10f ? my / r : 0.0f;
-      uz_o[c] = r > 1e-10f ? mz / r : 0.0f;
-    }
-    if (fill_solid) {
-#pragma unroll
-      for (int i = 0; i < kQ; ++i) Pop<S>::st(Po + p.plane[i], w_of(i), w_of(i));
-    }
+    for (int i = 0; i < kQ; ++i) Pop<S>::st(Pout + (c + p.plane[i]), w_of(i), w_of(i));
   }
-  if (!valid) return;
+}
 
-  // ------------------------------------------------------------------ thermal lattice
+// thermal lattice of any cell, with the cell's fluid velocity u (0 in solids)
+template <typename S, bool kOwn, bool kCoherent = false>
+__device__ __forceinline__ void thermal_cell(const uint32_t c, const S* __restrict__ Qin, S* __restrict__ Qout,
+                                             const float* __restrict__ qsrc, const float* __restrict__ T0,
+                                             const StepParams& p, const uint32_t lw, const float ux, const float uy,
+                                             const float uz) {
+  const int type = link_type(lw);
+  const S* __restrict__ Qc = Qin + c;  // outlet cells copy from Qc - 1
   const float Tb = p.T_ref;
   float G[kQ];
   float T;
   if (kOwn) {
-#define XAC_LD_G0(I) G[I] = Pop<S>::template ld<kCoherent>(Qc + p.plane[I], w_of(I) * Tb);
+#define XAC_LD_G0(I) G[I] = Pop<S>::template ld<kCoherent>(Qin + (c + p.plane[I]), w_of(I) * Tb);
     XAC_FOR19(XAC_LD_G0)
 #undef XAC_LD_G0
     T = kCoherent ? __ldcg(T0 + c) : __ldg(T0 + c);
@@ -268,11 +273,11 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
 #define XAC_LD_GFAST(I)                                                                                        \
   {                                                                                                            \
     if (ex_of(I) == 1)                                                                                         \
-      G[I] = (lw & kXLoBit) ? w_of(I) * p.T_in : Pop<S>::template ld<kCoherent>(Qc + p.pull[I], w_of(I) * Tb);                     \
+      G[I] = (lw & kXLoBit) ? w_of(I) * p.T_in : Pop<S>::template ld<kCoherent>(Qin + (c + p.pull[I]), w_of(I) * Tb);                     \
     else if (ex_of(I) == -1)                                                                                   \
-      G[I] = (lw & kXHiBit) ? Pop<S>::template ld<kCoherent>(Qc + p.plane[I], w_of(I) * Tb) : Pop<S>::template ld<kCoherent>(Qc + p.pull[I], w_of(I) * Tb); \
+      G[I] = (lw & kXHiBit) ? Pop<S>::template ld<kCoherent>(Qin + (c + p.plane[I]), w_of(I) * Tb) : Pop<S>::template ld<kCoherent>(Qin + (c + p.pull[I]), w_of(I) * Tb); \
     else                                                                                                       \
-      G[I] = Pop<S>::template ld<kCoherent>(Qc + p.pull[I], w_of(I) * Tb);                                                         \
+      G[I] = Pop<S>::template ld<kCoherent>(Qin + (c + p.pull[I]), w_of(I) * Tb);                                                         \
   }
       XAC_FOR19(XAC_LD_GFAST)
 #undef XAC_LD_GFAST
@@ -286,11 +291,11 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
     if (xlo)                                                                                                   \
       G[I] = w_of(I) * p.T_in;                                                                                 \
     else if (xhi)                                                                                              \
-      G[I] = Pop<S>::template ld<kCoherent>(Qc + p.plane[I], w_of(I) * Tb);                                                        \
+      G[I] = Pop<S>::template ld<kCoherent>(Qin + (c + p.plane[I]), w_of(I) * Tb);                                                        \
     else if (wall)                                                                                             \
-      G[I] = Pop<S>::template ld<kCoherent>(Qc + p.plane[opp_of(I)], w_of(I) * Tb);                                                \
+      G[I] = Pop<S>::template ld<kCoherent>(Qin + (c + p.plane[opp_of(I)]), w_of(I) * Tb);                                                \
     else                                                                                                       \
-      G[I] = Pop<S>::template ld<kCoherent>(Qc + p.pull[I], w_of(I) * Tb);                                                         \
+      G[I] = Pop<S>::template ld<kCoherent>(Qin + (c + p.pull[I]), w_of(I) * Tb);                                                         \
   }
       XAC_FOR19(XAC_LD_GSLOW)
 #undef XAC_LD_GSLOW
@@ -311,10 +316,29 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restri
     const float ge = feq_term(w_of(I) * T, edotu<I>(ux, uy, uz), usq15t);       \
     float v = G[I] - omega_t * (G[I] - ge);                                      \
     if (q > 0.0f) v += (w_of(I) * srcf) * q;                                     \
-    Pop<S>::st(Qo + p.plane[I], v, w_of(I) * Tb);                                \
+    Pop<S>::st(Qout + (c + p.plane[I]), v, w_of(I) * Tb);                                \
   }
   XAC_FOR19(XAC_TCOLLIDE)
 #undef XAC_TCOLLIDE
+}
+
+template <typename S, bool kMacro, bool kOwn, bool kCoherent = false>
+__device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restrict__ Pin, S* __restrict__ Pout,
+                                             const S* __restrict__ Qin, S* __restrict__ Qout,
+                                             const uint32_t* __restrict__ link, const float* __restrict__ qsrc,
+                                             const float* __restrict__ u_in_ptr, float* __restrict__ rho_o,
+                                             float* __restrict__ ux_o, float* __restrict__ uy_o,
+                                             float* __restrict__ uz_o, const float* __restrict__ T0,
+                                             const StepParams& p, const bool valid, const uint32_t lw,
+                                             const bool fill_solid) {
+  const bool fluid = valid && link_type(lw) != kSolid;
+  float ux = 0.0f, uy = 0.0f, uz = 0.0f;
+  if (fluid)
+    fluid_cell<S, kMacro, kCoherent>(c, Pin, Pout, u_in_ptr, rho_o, ux_o, uy_o, uz_o, p, lw, ux, uy, uz);
+  else if (valid)
+    solid_cell<S, kMacro, kCoherent>(c, Pin, Pout, rho_o, ux_o, uy_o, uz_o, p, fill_solid);
+  if (!valid) return;
+  thermal_cell<S, kOwn, kCoherent>(c, Qin, Qout, qsrc, T0, p, lw, ux, uy, uz);
 }
 
 // kCells cells per thread, at a stride of one block, so each load instruction stays coalesced.
@@ -338,6 +362,72 @@ __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__
     coupled_cell<S, kMacro, kOwn>(c, Pin, Pout, Qin, Qout, link, qsrc, u_in_ptr, rho_o, ux_o, uy_o, uz_o, T0, p,
                                   valid, lw, (fluid_lanes & sector_group<S>(lane)) != 0u);
   }
+}
+
+// ---- pair-compacted step ------------------------------------------------------------------------
+// A warp owns 64 consecutive cells, two groups of 32. When the two groups hold at most 32 non-solid cells
+// between them (the usual case in a porous design), the fluid lattice of all of them runs in ONE pass over a
+// compacted list - lane l takes the l-th non-solid cell - instead of two passes with the solid lanes idle. Each
+// lane then gets its own cells' velocities back by shuffles and runs the thermal lattice of its two cells.
+// Every cell runs exactly the arithmetic of coupled_cell, so results are identical.
+template <typename S, bool kMacro, bool kOwn>
+__global__ void __launch_bounds__(256) coupled_pair_kernel(const S* __restrict__ Pin, S* __restrict__ Pout,
+                                                           const S* __restrict__ Qin, S* __restrict__ Qout,
+                                                           const uint32_t* __restrict__ link,
+                                                           const float* __restrict__ qsrc,
+                                                           const float* __restrict__ u_in_ptr,
+                                                           float* __restrict__ rho_o, float* __restrict__ ux_o,
+                                                           float* __restrict__ uy_o, float* __restrict__ uz_o,
+                                                           const float* __restrict__ T0, StepParams p) {
+  __shared__ uint8_t slot[8][32];  // per warp: lane l of the compacted pass works on cell base + slot[l]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t base = (blockIdx.x * (blockDim.x >> 5) + warp) * 64u;
+  const uint32_t ncell = (uint32_t)p.g.ncell;
+  const uint32_t c0 = base + lane, c1 = base + 32u + lane;
+  const bool v0 = c0 < ncell, v1 = c1 < ncell;
+  const uint32_t solid_word = (uint32_t)kSolid << kTypeShift;
+  const uint32_t lw0 = v0 ? __ldg(link + c0) : solid_word, lw1 = v1 ? __ldg(link + c1) : solid_word;
+  const bool f0 = v0 && link_type(lw0) != kSolid, f1 = v1 && link_type(lw1) != kSolid;
+  const unsigned m0 = __ballot_sync(0xffffffffu, f0), m1 = __ballot_sync(0xffffffffu, f1);
+  const int k0 = __popc(m0), k1 = __popc(m1);
+  float ux0 = 0.0f, uy0 = 0.0f, uz0 = 0.0f, ux1 = 0.0f, uy1 = 0.0f, uz1 = 0.0f;
+  if (k0 + k1 <= 32) {
+    const unsigned below = (1u << lane) - 1u;
+    const int r0 = __popc(m0 & below), r1 = k0 + __popc(m1 & below);
+    if (f0) slot[warp][r0] = (uint8_t)lane;
+    if (f1) slot[warp][r1] = (uint8_t)(32 + lane);
+    __syncwarp();
+    const bool work = lane < k0 + k1;
+    const int src = work ? slot[warp][lane] : 0;
+    const uint32_t a = __shfl_sync(0xffffffffu, lw0, src & 31), b = __shfl_sync(0xffffffffu, lw1, src & 31);
+    float ux = 0.0f, uy = 0.0f, uz = 0.0f;
+    if (work)
+      fluid_cell<S, kMacro>(base + (uint32_t)src, Pin, Pout, u_in_ptr, rho_o, ux_o, uy_o, uz_o, p, src < 32 ? a : b,
+                            ux, uy, uz);
+    const float a0 = __shfl_sync(0xffffffffu, ux, r0 & 31), a1 = __shfl_sync(0xffffffffu, uy, r0 & 31),
+                a2 = __shfl_sync(0xffffffffu, uz, r0 & 31);
+    const float b0 = __shfl_sync(0xffffffffu, ux, r1 & 31), b1 = __shfl_sync(0xffffffffu, uy, r1 & 31),
+                b2 = __shfl_sync(0xffffffffu, uz, r1 & 31);
+    if (f0) {
+      ux0 = a0;
+      uy0 = a1;
+      uz0 = a2;
+    }
+    if (f1) {
+      ux1 = b0;
+      uy1 = b1;
+      uz1 = b2;
+    }
+    __syncwarp();
+  } else {
+    if (f0) fluid_cell<S, kMacro>(c0, Pin, Pout, u_in_ptr, rho_o, ux_o, uy_o, uz_o, p, lw0, ux0, uy0, uz0);
+    if (f1) fluid_cell<S, kMacro>(c1, Pin, Pout, u_in_ptr, rho_o, ux_o, uy_o, uz_o, p, lw1, ux1, uy1, uz1);
+  }
+  const unsigned sg = sector_group<S>(lane);
+  if (v0 && !f0) solid_cell<S, kMacro>(c0, Pin, Pout, rho_o, ux_o, uy_o, uz_o, p, (m0 & sg) != 0u);
+  if (v1 && !f1) solid_cell<S, kMacro>(c1, Pin, Pout, rho_o, ux_o, uy_o, uz_o, p, (m1 & sg) != 0u);
+  if (v0) thermal_cell<S, kOwn>(c0, Qin, Qout, qsrc, T0, p, lw0, ux0, uy0, uz0);
+  if (v1) thermal_cell<S, kOwn>(c1, Qin, Qout, qsrc, T0, p, lw1, ux1, uy1, uz1);
 }
 
 // ---- class-grouped step -------------------------------------------------------------------------

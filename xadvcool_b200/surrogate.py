@@ -63,6 +63,13 @@ def conv_weight_grad(x: torch.Tensor, dy: torch.Tensor, ksize: int, with_bias: b
     return dw, db
 
 
+def kernel_status() -> int:
+    """Reads and clears the convolution kernels' device status (0: every bounded wait completed)."""
+    v = C.c_int()
+    _capi.call("xac_conv3d_status", C.byref(v))
+    return int(v.value)
+
+
 def adjoint_weights(w_bf: torch.Tensor) -> torch.Tensor:
     """Weights of the data gradient: flipped taps, input and output channels swapped."""
     return w_bf.flip(0).transpose(1, 2).contiguous()
