@@ -231,6 +231,31 @@ def run_reference_arm(args):
 
 
 # ------------------------------------------------------------------------------------------------ GPU
+STEP_KERNELS = {0: "coupled_step_kernel<float>", 1: "coupled_step_grouped_kernel<float>",
+                2: "coupled_pair_kernel<float>"}
+
+
+def warm_start_probe(n_designs=16, tol=TOL):
+    """Seconds per converged design, surrogate warm start + batched solve vs cold batched solve (outside the timed
+    region): held-out gyroid seeds whose cold start passes the divergence guard, solved to the residual tolerance,
+    each batch timed from mask upload to every design's scalars (inference included)."""
+    from xadvcool_b200 import surrogate as S, warmstart as W
+    try:
+        model = S.load_pretrained("cuda")
+    except FileNotFoundError as e:
+        return {"unavailable": str(e)}
+    seeds = [W.HELDOUT_SEED0 + i for i in range(n_designs)]
+    r = W.compare_batched(model, seeds, max_steps=150000, tol=tol)
+    return {"designs": n_designs, "screened_out": r["screened_out"], "tol": tol,
+            "cold_s_per_converged_design": round(r["cold"]["s_per_converged_design"], 4),
+            "warm_s_per_converged_design": round(r["warm"]["s_per_converged_design"], 4),
+            "speedup": round(r["speedup"], 3), "step_ratio": round(r["step_ratio"], 3),
+            "cold_converged": r["cold"]["converged"], "warm_converged": r["warm"]["converged"],
+            "dP_rel_max": r["dP_rel_max"], "Rth_rel_max": r["Rth_rel_max"], "Rth_rel_median": r["Rth_rel_median"],
+            "within_half_percent": r["within_half_percent"], "compared": r["compared"],
+            "cold_tripped_solved_warm": r.get("warm_cold_tripped", {}).get("converged")}
+
+
 def forms_probe(dev, mask, lat_kw, shape):
     """Side measurements of the other forms on the same GPU (outside the timed region): FP16 / BF16 population
     storage on the same design, and the persistent batched solve of 64 mixed designs (1000 steps)."""
@@ -259,6 +284,7 @@ def forms_probe(dev, mask, lat_kw, shape):
     b.close()
     out["batch64_mixed_mlups"] = round(cells * 1000 / dt / 1e6, 1)
     out["batch64_cells"] = cells
+    out["warm_start"] = warm_start_probe()
     return out
 
 
@@ -352,7 +378,7 @@ def run_gpu_arm(args):
                 "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                              "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                              "traffic": (round(tpc * cells) if tpc else None),
-                             "kernel": "coupled_step_kernel<float>",
+                             "kernel": STEP_KERNELS[shape["variant"]],
                              "alg_bytes_per_launch": alg_bytes, "mean_launch_us": round(step_ms * 1e3, 3)},
                 "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "s_per_converged_design": round(e2e_max, 4),

@@ -79,3 +79,16 @@ def test_features_layout():
     assert float(x[0, ..., 1].max()) == 1.0
     assert torch.allclose(x[0, ..., 2].float(), torch.tensor(20 * u_in).to(S.BF16).float())
     assert (x[0, ..., 3:] == 0).all()
+
+
+def test_trained_weights_load_and_run_cpu():
+    """The committed weights load and give finite outputs (the network is fully convolutional: any volume whose
+    sides divide by 8 runs; a small one keeps this quick on the CPU)."""
+    m = S.load_pretrained("cpu")
+    assert m.norm is not None
+    x = torch.zeros(1, 8, 16, 24, 16)
+    x[..., 0] = 1.0
+    x[0, 0, :, :, 1] = 1.0
+    x[..., 2] = 0.6
+    y = m.forward(x.to(S.BF16), S.torch_conv3d)
+    assert y.shape == (1, 8, 16, 24, 16) and torch.isfinite(y).all()

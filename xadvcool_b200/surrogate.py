@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+from pathlib import Path
 
 import numpy as np
 import torch
@@ -206,6 +207,25 @@ class Surrogate:
             self.params[k] = v.to(self.device).requires_grad_(True)
         if "norm.mean" in sd:
             self.norm = (sd["norm.mean"].to(self.device), sd["norm.std"].to(self.device))
+
+
+WEIGHTS = Path(__file__).resolve().parent / "weights" / "surrogate_gyroid148.pt"
+
+
+def save_weights(model: Surrogate, path=WEIGHTS):
+    """Convolution weights in BF16 (the precision the kernels read them in), everything else in FP32."""
+    sd = {k: (v.to(BF16) if k.endswith(".w") else v) for k, v in model.state_dict().items()}
+    Path(path).parent.mkdir(parents=True, exist_ok=True)
+    torch.save(sd, path)
+
+
+def load_pretrained(device="cuda", path=WEIGHTS) -> Surrogate:
+    """The surrogate trained on the seeded 148x128x32 gyroid cold plates (python -m xadvcool_b200.warmstart)."""
+    if not Path(path).exists():
+        raise FileNotFoundError(f"no trained surrogate weights at {path}")
+    m = Surrogate(device)
+    m.load_state_dict({k: (v.float() if k.endswith(".w") else v) for k, v in torch.load(path).items()})
+    return m
 
 
 # ------------------------------------------------------------------------------------------------ data
