@@ -203,10 +203,8 @@ int xac_lattice_set_inlet(xac_lattice *lat, double u_inlet, void *stream);
 int xac_lattice_get_inlet(xac_lattice *lat, double *u_inlet, void *stream);
 int xac_lattice_steps_done(const xac_lattice *lat, long long *steps);
 /* Launch shape of the fused step kernel: threads per block (64, 128, 256) and the visiting order:
- * variant 0 = one thread per cell in memory order; variant 1 = cells grouped by class (bulk fluid, bulk solid,
- * inlet/outlet/y-z-face cells) so that a warp never mixes the fluid and thermal-only work; variant 2 = a warp owns
- * 64 cells and runs the fluid lattice of their non-solid cells in one compacted pass when they are at most 32.
- * Results do not depend on it (every cell runs the same arithmetic); xadvcool_b200.autotune picks it. */
+ * variant must be 0 (one thread per row position, in memory order). Results do not depend on the block size (every
+ * cell runs the same arithmetic); xadvcool_b200.autotune picks it. */
 int xac_lattice_tune(xac_lattice *lat, int block, int variant);
 int xac_lattice_get_tune(const xac_lattice *lat, int *block, int *variant);
 /* Inputs of generate_dataset.py:80 compute_macroscopic_metrics that are not fields. */

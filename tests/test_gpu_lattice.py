@@ -201,25 +201,36 @@ def test_16bit_storage_error_vs_fp64_oracle(precision, tol_u, tol_T, cuda):
 @pytest.mark.parametrize("precision", ["fp32", "fp16", "bf16"])
 @pytest.mark.parametrize("block", [64, 128, 256])
 def test_launch_shapes_give_identical_bits(precision, block, cuda):
-    """Memory-order, class-grouped and pair-compacted visiting orders at every block size: same bits (and the
-    oracle's). The design has both porous stretches (compacted fluid pass) and all-fluid buffers (two passes)."""
+    """Every block size, on a lattice whose row length (48 -> pitch 64) has a compile-time instantiation and on one
+    (nx = 300) that takes the runtime-pitch kernel: same bits as the default shape, and the oracle's."""
     mask, hs, u_in, _ = designs.gyroid_design(3, nx=48, ny=20, nz=12)
     kw = dict(heat_source=hs, tau_fluid=0.56, u_inlet_val=u_in, heat_power=0.05, precision=precision)
     out = {}
-    for variant in (0, 1, 2):
+    for key, b in (("default", 128), ("tuned", block)):
         lat = Lattice(mask, **kw)
-        lat.tune(block, variant)
-        assert lat.get_tune() == (block, variant)
+        lat.tune(b, 0)
+        assert lat.get_tune() == (b, 0)
         lat.step(37)
-        out[variant] = [t.cpu().numpy() for t in lat.fields()] + [lat.stats()]
+        out[key] = [t.cpu().numpy() for t in lat.fields()] + [lat.stats()]
         lat.close()
-    for v in (1, 2):
-        for a, b in zip(out[0], out[v]):
-            assert np.array_equal(a, b)
+    for a, b in zip(out["default"], out["tuned"]):
+        assert np.array_equal(a, b)
     if precision == "fp32":
         ref = oracle_fields(mask, 37, hs=hs, tau_fluid=0.56, u_inlet_val=u_in, heat_power=0.05)
-        assert_exact(ref, *out[1][:3])
-        assert_exact(ref, *out[2][:3])
+        assert_exact(ref, *out["tuned"][:3])
+
+
+@pytest.mark.parametrize("nx", [20, 33, 100, 300])
+def test_row_lengths_match_oracle(nx, cuda):
+    """Row lengths 32, 64, 128 (compile-time) and 320 (runtime pitch), ragged x padding: bit-exact FP32."""
+    mask, hs, u_in, _ = designs.gyroid_design(5, nx=nx, ny=9, nz=7, buf=4)
+    kw = dict(heat_source=hs, tau_fluid=0.57, u_inlet_val=u_in, heat_power=0.05)
+    lat = Lattice(mask, **kw)
+    lat.step(23)
+    got = [t.cpu().numpy() for t in lat.fields()]
+    lat.close()
+    ref = oracle_fields(mask, 23, hs=hs, tau_fluid=0.57, u_inlet_val=u_in, heat_power=0.05)
+    assert_exact(ref, *got)
 
 
 def test_tune_rejects_bad_shapes(cuda):
@@ -227,7 +238,7 @@ def test_tune_rejects_bad_shapes(cuda):
     with pytest.raises(Exception):
         lat.tune(96, 0)
     with pytest.raises(Exception):
-        lat.tune(128, 3)
+        lat.tune(128, 1)
 
 
 def test_autotune_picks_a_valid_shape_without_touching_results(cuda, tmp_path, monkeypatch):

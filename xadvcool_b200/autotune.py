@@ -15,7 +15,7 @@ import numpy as np
 import torch
 
 BLOCKS = (64, 128, 256)
-VARIANTS = (0, 1, 2)  # 0: memory order, 1: grouped by cell class, 2: pair-compacted fluid pass
+VARIANTS = (0,)  # one visiting order (row positions in memory order)
 
 
 def _cache_path() -> Path:

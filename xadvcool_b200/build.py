@@ -6,6 +6,7 @@ bit against a CPU restatement compiled the same way.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -24,6 +25,9 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "--expt-r
 UNITS = [
     ("ops_reference_layout.cu", ["--fmad=false"]),
     ("lattice.cu", ["--fmad=false"]),
+    ("step_f32.cu", ["--fmad=false"]),
+    ("step_f16.cu", ["--fmad=false"]),
+    ("step_bf16.cu", ["--fmad=false"]),
     ("stats_noalloc.cu", ["--fmad=false"]),
     ("conv3d.cu", []),
 ]
@@ -47,15 +51,19 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     nvcc = _nvcc()
     BUILD.mkdir(exist_ok=True)
     headers = list(CSRC.glob("*.cuh")) + [PKG.parent / "include" / "xac.h"]
-    objs = []
+    objs, jobs = [], []
     for src, extra in UNITS:
         obj = BUILD / (Path(src).stem + ".o")
         objs.append(obj)
         if force or _stale(obj, [CSRC / src] + headers):
-            cmd = [nvcc, *COMMON, *extra, "-c", str(CSRC / src), "-o", str(obj)]
+            jobs.append([nvcc, *COMMON, *extra, "-c", str(CSRC / src), "-o", str(obj)])
+    # units compile independently: run them side by side
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for cmd in jobs:
             if verbose:
                 print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+        for f in [ex.submit(subprocess.run, cmd, check=True) for cmd in jobs]:
+            f.result()
     if force or _stale(LIB, objs):
         cmd = [nvcc, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
         if verbose:

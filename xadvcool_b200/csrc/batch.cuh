@@ -88,48 +88,23 @@ __device__ __forceinline__ int find_slot(const uint32_t* prefix, int n, uint32_t
   return lo;
 }
 
-template <typename S>
-__device__ __forceinline__ float finalize_T_cell(const BatchDesign& d, const S* __restrict__ Qin, uint32_t c) {
-  const uint32_t lw = __ldg(d.link + c);
-  const int type = link_type(lw);
-  const StepParams& p = d.p;
-  const float Tb = p.T_ref;
-  const S* __restrict__ Qc = Qin + c;
-  float T = 0.0f;
-  if (type == kInlet) {
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) T += w_of(i) * p.T_in;
-  } else if (type == kOutlet) {
-    const S* __restrict__ Qs = (lw & kXLoBit) ? Qc : Qc - 1;
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) T += Pop<S>::template ld<true>(Qs + p.plane[i], w_of(i) * Tb);
-  } else {
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) {
-      const bool xlo = ex_of(i) == 1 && (lw & kXLoBit);
-      const bool xhi = ex_of(i) == -1 && (lw & kXHiBit);
-      const bool wall = (lw & wall_bits(i)) != 0u;
-      float v;
-      if (xlo) v = w_of(i) * p.T_in;
-      else if (xhi) v = Pop<S>::template ld<true>(Qc + p.plane[i], w_of(i) * Tb);
-      else if (wall) v = Pop<S>::template ld<true>(Qc + p.plane[opp_of(i)], w_of(i) * Tb);
-      else v = Pop<S>::template ld<true>(Qc + p.pull[i], w_of(i) * Tb);
-      T += v;
-    }
-  }
-  return T;
-}
-
+// tile = blockDim consecutive row positions (rows of `pitch` positions, x >= nx padding), one per thread
 template <typename S, bool kMacro, bool kOwn>
 __device__ __forceinline__ void batch_step_tile(const BatchDesign& d, uint32_t tile, int cur) {
-  const uint32_t c = tile * blockDim.x + threadIdx.x;
-  const bool valid = c < d.ncell;
+  const uint32_t pos = tile * blockDim.x + threadIdx.x;
+  const uint32_t pitch = (uint32_t)d.p.g.pitch;
+  const uint32_t r = pos / pitch, x = pos - r * pitch;
+  if (r >= (uint32_t)d.p.g.rows) return;  // whole warps (the pitch is a multiple of 32)
+  const bool valid = x < (uint32_t)d.p.g.nx;
+  const uint32_t c = r * (uint32_t)d.p.g.nx + x;
   const uint32_t lw = valid ? __ldg(d.link + c) : ((uint32_t)kSolid << kTypeShift);
   const unsigned fluid_lanes = __ballot_sync(0xffffffffu, valid && link_type(lw) != kSolid);
   const int lane = threadIdx.x & 31;
-  coupled_cell<S, kMacro, kOwn, true>(c, (const S*)d.P[cur], (S*)d.P[cur ^ 1], (const S*)d.Q[cur], (S*)d.Q[cur ^ 1],
-                                d.link, d.qsrc, d.u_in, d.rho, d.ux, d.uy, d.uz, d.T, d.p, valid, lw,
-                                (fluid_lanes & sector_group<S>(lane)) != 0u);
+  coupled_cell<S, kMacro, kOwn, true, 0>(c, pop_base(r, x, d.p.g, (int)pitch), (const S*)d.P[cur], (S*)d.P[cur ^ 1],
+                                         (const S*)d.Q[cur], (S*)d.Q[cur ^ 1], d.qsrc, d.u_in, d.rho, d.ux, d.uy,
+                                         d.uz, d.T, d.p, valid, lw, (fluid_lanes & sector_group<S>(lane)) != 0u);
+  pad_fill<S, 0>(valid, fluid_lanes, __ballot_sync(0xffffffffu, valid), lane, (S*)d.P[cur ^ 1], (S*)d.Q[cur ^ 1],
+                 pop_base(r, x, d.p.g, (int)pitch), d.p.g);
 }
 
 struct BatchRun {
@@ -142,7 +117,7 @@ struct BatchRun {
 
 template <typename S>
 #ifndef XAC_BATCH_MIN_BLOCKS
-#define XAC_BATCH_MIN_BLOCKS 4
+#define XAC_BATCH_MIN_BLOCKS 3
 #endif
 __global__ void __launch_bounds__(256, XAC_BATCH_MIN_BLOCKS) batch_persistent_kernel(BatchDesign* __restrict__ D, BatchCtl* __restrict__ ctl,
                                                                double* __restrict__ rows, BatchRun run) {
@@ -195,7 +170,7 @@ __global__ void __launch_bounds__(256, XAC_BATCH_MIN_BLOCKS) batch_persistent_ke
         const S* Qnew = (const S*)d.Q[cur ^ 1];
         for (uint32_t c = tile * kStatsTile + threadIdx.x; c < (tile + 1) * kStatsTile && c < d.ncell;
              c += blockDim.x)
-          d.T[c] = finalize_T_cell<S>(d, Qnew, c);
+          d.T[c] = finalize_T_cell<S, true>(Qnew, d.link, d.p, c);
         __syncthreads();
         FieldView v{};
         v.rho = d.rho;

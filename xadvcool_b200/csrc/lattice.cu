@@ -39,9 +39,8 @@ __device__ __forceinline__ long long ref_index(int x, int y, int z, int ny, int 
   return ((long long)x * ny + y) * nz + z;
 }
 
-// sector = cells per 32-byte DRAM sector of a population plane (8 for FP32, 16 for 16-bit storage)
 __global__ void build_link_kernel(const uint8_t* __restrict__ type, const float* __restrict__ qsrc,
-                                  uint32_t* __restrict__ link, Geom g, int sector) {
+                                  uint32_t* __restrict__ link, Geom g) {
   const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (c >= g.ncell) return;
   const int x = (int)(c % g.nx);
@@ -64,14 +63,6 @@ __global__ void build_link_kernel(const uint8_t* __restrict__ type, const float*
   if (z == 0) w |= kZLoBit;
   if (z == g.nz - 1) w |= kZHiBit;
   if (w & (kYLoBit | kYHiBit | kZLoBit | kZHiBit)) w |= kYZBit;
-  if (type[c] == kSolid) {
-    const long long s0 = c - c % sector;
-    for (long long k = s0; k < s0 + sector && k < g.ncell; ++k)
-      if (type[k] != kSolid) {
-        w |= kFillBit;
-        break;
-      }
-  }
   link[c] = w;
 }
 
@@ -103,7 +94,9 @@ __global__ void init_state_kernel(const float* __restrict__ rho, const float* __
                                   S* __restrict__ P1, S* __restrict__ Q0, StepParams p) {
   const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (c >= p.g.ncell) return;
-  const long long N = p.g.N;
+  const int RL = p.g.pitch;
+  const uint32_t row = (uint32_t)(c / p.g.nx), x = (uint32_t)(c - (long long)row * p.g.nx);
+  const long long e0 = pop_base(row, x, p.g, RL);
   const float r = rho[c], vx = ux[c], vy = uy[c], vz = uz[c];
   const bool solid = type[c] == kSolid;
   const float usq15 = 1.5f * ((vx * vx + vy * vy) + vz * vz);
@@ -115,10 +108,10 @@ __global__ void init_state_kernel(const float* __restrict__ rho, const float* __
   {                                                                                   \
     const float fe = feq_term(w_of(I) * r, edotu<I>(vx, vy, vz), usq15);             \
     const float pc = solid ? fe : fe - omega * (fe - fe);                             \
-    Pop<S>::st(P0 + (long long)I * N + c, pc, w_of(I));                               \
-    Pop<S>::st(P1 + (long long)I * N + c, pc, w_of(I));                               \
+    Pop<S>::st(P0 + e0 + (long long)I * RL, pc, w_of(I));                            \
+    Pop<S>::st(P1 + e0 + (long long)I * RL, pc, w_of(I));                            \
     const float ge = feq_term(w_of(I) * Tc, edotu<I>(tx, ty, tz), usq15t);           \
-    Pop<S>::st(Q0 + (long long)I * N + c, ge, w_of(I) * p.T_ref);                     \
+    Pop<S>::st(Q0 + e0 + (long long)I * RL, ge, w_of(I) * p.T_ref);                  \
   }
   XAC_FOR19(XAC_INIT)
 #undef XAC_INIT
@@ -180,9 +173,7 @@ struct LatticeImpl {
   float relax[5] = {1.0f, 1.0f, 1.0f, 0.5f, 0.5f};  // omega_f, omega_tf, omega_ts, srcf_f, srcf_s (device-computed)
   float u_in_host = 0.0f;
   int tune_block = 128;  // threads per block of the step kernel
-  int tune_variant = 0;  // 0: cells in memory order; 1: cells grouped by class; 2: pair-compacted fluid pass
-  uint32_t* cells = nullptr;                 // class-grouped cell list (kNoCell padding)
-  uint32_t cells_len = 0, end_fluid = 0, end_solid = 0;
+  int tune_variant = 0;  // one visiting order (row positions in memory order); kept for the ABI
 
   void* P[2] = {nullptr, nullptr};
   void* Qb[2] = {nullptr, nullptr};
@@ -227,12 +218,6 @@ struct LatticeImpl {
     p.omega_ts = relax[2];
     p.srcf_f = relax[3];
     p.srcf_s = relax[4];
-    const long long nxy = (long long)g.nx * g.ny;
-    for (int i = 0; i < kQ; ++i) {
-      const long long off = ex_of(i) + (long long)ey_of(i) * g.nx + (long long)ez_of(i) * nxy;
-      p.plane[i] = (int32_t)((long long)i * g.N);
-      p.pull[i] = (int32_t)((long long)i * g.N - off);
-    }
     return p;
   }
 
@@ -241,7 +226,6 @@ struct LatticeImpl {
     for (void* b : {P[0], P[1], Qb[0], Qb[1]}) cudaFree(b);
     cudaFree(type);
     cudaFree(link);
-    cudaFree(cells);
     cudaFree(qsrc);
     cudaFree(u_in);
     cudaFree(rho);
@@ -262,36 +246,8 @@ struct LatticeImpl {
     S* Pout = (S*)P[cur ^ 1];
     const S* Qin = (const S*)Qb[cur];
     S* Qout = (S*)Qb[cur ^ 1];
-    const int b = tune_block;
-    if (tune_variant == 1) {
-      const unsigned grid = cells_len / b;
-#define XAC_LAUNCH(M, O)                                                                                   \
-  coupled_step_grouped_kernel<S, M, O><<<grid, b, 0, s>>>(cells, end_fluid, end_solid, Pin, Pout, Qin, Qout, \
-                                                          link, qsrc, u_in, rho, ux, uy, uz, T, p)
-      if (macro && own) XAC_LAUNCH(true, true);
-      else if (macro) XAC_LAUNCH(true, false);
-      else if (own) XAC_LAUNCH(false, true);
-      else XAC_LAUNCH(false, false);
-#undef XAC_LAUNCH
-    } else if (tune_variant == 2) {
-      const unsigned grid = grid_for(g.ncell, 2 * b);  // 64 cells per warp
-#define XAC_LAUNCH(M, O) \
-  coupled_pair_kernel<S, M, O><<<grid, b, 0, s>>>(Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux, uy, uz, T, p)
-      if (macro && own) XAC_LAUNCH(true, true);
-      else if (macro) XAC_LAUNCH(true, false);
-      else if (own) XAC_LAUNCH(false, true);
-      else XAC_LAUNCH(false, false);
-#undef XAC_LAUNCH
-    } else {
-      const unsigned grid = grid_for(g.ncell, b);
-#define XAC_LAUNCH(M, O) \
-  coupled_step_kernel<S, M, O, 1><<<grid, b, 0, s>>>(Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux, uy, uz, T, p)
-      if (macro && own) XAC_LAUNCH(true, true);
-      else if (macro) XAC_LAUNCH(true, false);
-      else if (own) XAC_LAUNCH(false, true);
-      else XAC_LAUNCH(false, false);
-#undef XAC_LAUNCH
-    }
+    StepLaunch a{Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux, uy, uz, T, p, tune_block, macro, own, s};
+    launch_coupled_step<S>(a);
     cur ^= 1;
     return XAC_OK;
   }
@@ -517,8 +473,8 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
   XAC_REQUIRE(d, "xac_lattice_create: null descriptor");
   XAC_REQUIRE(d->nx >= 3 && d->ny >= 1 && d->nz >= 1, "xac_lattice_create: lattice %d x %d x %d too small", d->nx,
               d->ny, d->nz);
-  XAC_REQUIRE((long long)d->nx * d->ny * d->nz * kQ < (1LL << 31),
-              "xac_lattice_create: lattice too large (19 x cells must stay below 2^31)");
+  XAC_REQUIRE(((long long)d->ny * d->nz + 2LL * (d->ny + 2)) * kQ * ((d->nx + 31) / 32 * 32) < (1LL << 31),
+              "xac_lattice_create: lattice too large (19 x padded cells must stay below 2^31)");
   XAC_REQUIRE(d->mask, "xac_lattice_create: null mask");
   XAC_REQUIRE(d->tau_fluid > 0.5, "xac_lattice_create: tau_fluid must exceed 0.5 (got %g)", d->tau_fluid);
   XAC_REQUIRE(d->Pr > 0, "xac_lattice_create: Pr must be positive");
@@ -530,7 +486,10 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
   L.g.ny = ny;
   L.g.nz = nz;
   L.g.ncell = n;
-  L.g.N = (n + 63) / 64 * 64;
+  L.g.pitch = (nx + 31) / 32 * 32;
+  L.g.rows = ny * nz;
+  L.g.guard = (long long)(ny + 2) * kQ * L.g.pitch;
+  L.g.N = (long long)L.g.rows * kQ * L.g.pitch + 2 * L.g.guard;
   L.precision = d->precision;
   L.pop_elem = d->precision == XAC_FP32 ? 4 : 2;
   L.tau_fluid = d->tau_fluid;
@@ -557,30 +516,7 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
         type[((size_t)z * ny + y) * nx + x] = (uint8_t)m;
       }
   std::vector<float> q = host_qsrc(d);
-  // class-grouped visiting order: bulk fluid, bulk solid, then inlet/outlet/y-z-face cells, each class in
-  // memory order and padded to a multiple of 512 entries
-  std::vector<uint32_t> lists[3];
-  for (int z = 0; z < nz; ++z)
-    for (int y = 0; y < ny; ++y)
-      for (int x = 0; x < nx; ++x) {
-        const uint32_t c = (uint32_t)(((size_t)z * ny + y) * nx + x);
-        const int m = type[c];
-        const bool face = y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
-        const int cls = face || m == kInlet || m == kOutlet ? kClassOther : (m == kSolid ? kClassBulkSolid
-                                                                                           : kClassBulkFluid);
-        lists[cls].push_back(c);
-      }
-  std::vector<uint32_t> cells;
-  uint32_t ends[3];
-  for (int k = 0; k < 3; ++k) {
-    cells.insert(cells.end(), lists[k].begin(), lists[k].end());
-    while (cells.size() % 512) cells.push_back(kNoCell);
-    ends[k] = (uint32_t)cells.size();
-  }
-  L.cells_len = (uint32_t)cells.size();
-  L.end_fluid = ends[0];
-  L.end_solid = ends[1];
-  const size_t pop_bytes = (size_t)kQ * L.g.N * L.pop_elem;
+  const size_t pop_bytes = (size_t)L.g.N * L.pop_elem;
   for (int b = 0; b < 2; ++b) {
     XAC_CUDA(cudaMalloc(&L.P[b], pop_bytes));
     XAC_CUDA(cudaMalloc(&L.Qb[b], pop_bytes));
@@ -588,7 +524,6 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
   int r;
   if ((r = dmalloc(&L.type, n, "alloc type")) != XAC_OK) return r;
   if ((r = dmalloc(&L.link, n, "alloc link")) != XAC_OK) return r;
-  if ((r = dmalloc(&L.cells, L.cells_len, "alloc cell list")) != XAC_OK) return r;
   if ((r = dmalloc(&L.qsrc, n, "alloc qsrc")) != XAC_OK) return r;
   if ((r = dmalloc(&L.u_in, 1, "alloc u_in")) != XAC_OK) return r;
   for (float** f : {&L.rho, &L.ux, &L.uy, &L.uz, &L.T})
@@ -600,18 +535,17 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
   }
   if ((r = dmalloc(&L.red_out, 64, "alloc red_out")) != XAC_OK) return r;
   XAC_CUDA(cudaMallocHost(&L.host_out, 64 * sizeof(double)));
-  // the pop planes' padding is never read, but keep it defined
+  // guards and row padding are never used as values; keep them defined
   for (int b = 0; b < 2; ++b) {
     XAC_CUDA(cudaMemsetAsync(L.P[b], 0, pop_bytes, s));
     XAC_CUDA(cudaMemsetAsync(L.Qb[b], 0, pop_bytes, s));
   }
   XAC_CUDA(cudaMemcpyAsync(L.type, type.data(), n, cudaMemcpyHostToDevice, s));
-  XAC_CUDA(cudaMemcpyAsync(L.cells, cells.data(), cells.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
   XAC_CUDA(cudaMemcpyAsync(L.qsrc, q.data(), n * sizeof(float), cudaMemcpyHostToDevice, s));
   set_scalar_kernel<<<1, 1, 0, s>>>(L.u_in, L.u_in_host);
   relaxation_factors_kernel<<<1, 1, 0, s>>>((float)L.tau_fluid, L.tau_th_f, L.tau_th_s, (float*)L.red_out);
   XAC_CUDA(cudaMemcpyAsync(L.relax, L.red_out, sizeof(L.relax), cudaMemcpyDeviceToHost, s));
-  build_link_kernel<<<grid_for(n, kBlock), kBlock, 0, s>>>(L.type, L.qsrc, L.link, L.g, 32 / (int)L.pop_elem);
+  build_link_kernel<<<grid_for(n, kBlock), kBlock, 0, s>>>(L.type, L.qsrc, L.link, L.g);
   XAC_CUDA(cudaGetLastError());
   // host vectors go out of scope: make the copies complete first
   XAC_CUDA(cudaStreamSynchronize(s));
@@ -738,7 +672,7 @@ int xac_lattice_tune(xac_lattice* lat, int block, int variant) {
   XAC_REQUIRE(lat, "xac_lattice_tune: null lattice");
   XAC_REQUIRE(block == 64 || block == 128 || block == 256, "xac_lattice_tune: block must be 64, 128 or 256 (got %d)",
               block);
-  XAC_REQUIRE(variant >= 0 && variant <= 2, "xac_lattice_tune: variant must be 0, 1 or 2 (got %d)", variant);
+  XAC_REQUIRE(variant == 0, "xac_lattice_tune: variant must be 0 (got %d)", variant);
   LatticeImpl& L = lat->impl;
   std::lock_guard<std::mutex> g(L.mu);
   if (L.tune_block != block || L.tune_variant != variant) {
@@ -782,7 +716,7 @@ int xac_lattice_scalars(xac_lattice* lat, const xac_scalar_params* prm, double* 
 int xac_lattice_state_bytes(const xac_lattice* lat, size_t* bytes) {
   XAC_REQUIRE(lat && bytes, "xac_lattice_state_bytes: null pointer");
   const LatticeImpl& L = lat->impl;
-  const size_t pop = (size_t)kQ * L.g.N * L.pop_elem;
+  const size_t pop = (size_t)L.g.N * L.pop_elem;
   *bytes = 64 + 2 * pop + 5 * (size_t)L.g.ncell * sizeof(float);
   return XAC_OK;
 }
@@ -802,7 +736,7 @@ int xac_lattice_save_state(xac_lattice* lat, void* host_dst, size_t bytes, void*
   std::memcpy(&hdr[7], &u_in, sizeof(float));
   char* dst = (char*)host_dst;
   std::memcpy(dst, hdr, 64);
-  const size_t pop = (size_t)kQ * L.g.N * L.pop_elem;
+  const size_t pop = (size_t)L.g.N * L.pop_elem;
   const size_t nf = (size_t)L.g.ncell * sizeof(float);
   XAC_CUDA(cudaMemcpyAsync(dst + 64, L.P[L.cur], pop, cudaMemcpyDeviceToHost, s));
   XAC_CUDA(cudaMemcpyAsync(dst + 64 + pop, L.Qb[L.cur], pop, cudaMemcpyDeviceToHost, s));
@@ -827,7 +761,7 @@ int xac_lattice_load_state(xac_lattice* lat, const void* host_src, size_t bytes,
   std::lock_guard<std::mutex> g(L.mu);
   cudaStream_t s = as_stream(stream);
   const char* src = (const char*)host_src;
-  const size_t pop = (size_t)kQ * L.g.N * L.pop_elem;
+  const size_t pop = (size_t)L.g.N * L.pop_elem;
   const size_t nf = (size_t)L.g.ncell * sizeof(float);
   // solid cells are read from either buffer, so both get the saved fluid populations
   XAC_CUDA(cudaMemcpyAsync(L.P[0], src + 64, pop, cudaMemcpyHostToDevice, s));
@@ -1183,7 +1117,7 @@ int xac_batch_run(xac_batch* b, const xac_run_opts* o, xac_run_result* res, void
     d.uz = L.uz;
     d.T = L.T;
     d.ncell = (uint32_t)L.g.ncell;
-    d.tiles = (uint32_t)((L.g.ncell + b->block - 1) / b->block);
+    d.tiles = (uint32_t)(((long long)L.g.rows * L.g.pitch + b->block - 1) / b->block);  // row positions
     d.stat_tiles = (uint32_t)stats_tiles(L.g.ncell);
     d.row_base = row;
     row += d.stat_tiles;

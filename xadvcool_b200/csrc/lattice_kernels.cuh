@@ -1,7 +1,13 @@
 // Device kernels of the fused lattice (internal layout).
 //
-// Internal layout: cell c = (z*ny + y)*nx + x (x fastest, the flow/streaming axis); populations are
-// structure-of-arrays planes pop[i*N + c], N = cell count rounded up to 64 (256-byte aligned planes).
+// Internal layout. Cells are numbered c = (z*ny + y)*nx + x (x fastest, the flow/streaming axis) for the link
+// words, the heat source and the macroscopic fields. Populations are stored row-tiled: a row (y, z) holds the 19
+// directions one after another, each a run of `pitch` = nx rounded up to 32 values:
+//     pop[guard + ((z*ny + y)*19 + i)*pitch + x]
+// so a direction's value of a row's neighbour in x, y or in the same row is at a compile-time distance
+// (i*pitch - ex - ey*19*pitch) from the cell, and only z neighbours need another base pointer (one slab of
+// ny*19*pitch values away). Rows of `guard` = (ny + 2)*19*pitch zero values before and after the array keep every
+// source address that a bounce-back lane might form inside the allocation.
 //
 // Scheme. Both lattices store POST-COLLISION populations and every step is one pull pass:
 //   fluid:   F^k(x)   = stream(P^{k-1})(x)  ->  rho^k, u^k  ->  P^k(x) = collide(F^k)
@@ -24,8 +30,6 @@ namespace xac {
 // bit  22    : heated (heat_source * heat_power > 0)
 // bit  23/24 : x == 0 / x == nx-1
 // bits 26..29: y == 0, y == ny-1, z == 0, z == nz-1; bit 25 = any of them
-// bit  30    : solid cell whose population sector also holds a non-solid cell (it stores w_i so that every
-//              fluid-output sector is written whole)
 // With these bits a step needs no integer division to locate a cell.
 constexpr int kTypeShift = 20;
 constexpr uint32_t kHeatedBit = 1u << 22;
@@ -36,7 +40,6 @@ constexpr uint32_t kYLoBit = 1u << 26;
 constexpr uint32_t kYHiBit = 1u << 27;
 constexpr uint32_t kZLoBit = 1u << 28;
 constexpr uint32_t kZHiBit = 1u << 29;
-constexpr uint32_t kFillBit = 1u << 30;  // solid cell sharing a 32-byte DRAM sector with a non-solid cell
 __device__ __forceinline__ int link_type(uint32_t lw) { return (int)((lw >> kTypeShift) & 3u); }
 
 // wall bits that make the thermal source of direction I leave the domain through a y/z face
@@ -48,8 +51,21 @@ __host__ __device__ constexpr uint32_t wall_bits(int I) {
 struct Geom {
   int nx, ny, nz;
   long long ncell;  // nx*ny*nz
-  long long N;      // population plane stride (elements)
+  int pitch;        // population row length: nx rounded up to 32
+  int rows;         // ny*nz
+  long long guard;  // zero elements before the first and after the last row of a population array
+  long long N;      // elements of one population array: rows*19*pitch + 2*guard
 };
+
+// row length, a compile-time constant when kT > 0
+template <int kT>
+__host__ __device__ __forceinline__ int row_len(const Geom& g) {
+  return kT > 0 ? kT : g.pitch;
+}
+// element of (direction 0, this row, x) for compact cell (row r, x)
+__device__ __forceinline__ uint32_t pop_base(uint32_t r, uint32_t x, const Geom& g, int pitch) {
+  return (uint32_t)g.guard + r * (uint32_t)(kQ * pitch) + x;
+}
 
 // ---- population storage -------------------------------------------------------------------
 // FP32 stores the population itself. The 16-bit forms store the deviation from the rest
@@ -97,15 +113,32 @@ struct StepParams {
   // 1/tau and 1 - omega/2 computed once on the device (the same IEEE float division as in the reference's
   // kernels, hoisted out of the per-cell work): fluid omega, thermal omega fluid/solid, source factor fluid/solid
   float omega_f, omega_tf, omega_ts, srcf_f, srcf_s;
-  // element offsets: plane[i] = i*N; pull[i] = i*N - (ex + ey*nx + ez*nx*ny), so that the source of direction i
-  // for cell c is pop[c + pull[i]] and its own value is pop[c + plane[i]] (32-bit indices: all are below 19 N).
-  int32_t plane[kQ];
-  int32_t pull[kQ];
 };
+
+// One cell's view of a population array: the cell's own position (direction 0) and the same x in the rows one
+// z-slab below (source of directions with ez = +1) and above (ez = -1).
+template <typename S>
+struct Rows {
+  const S* c;
+  const S* zm;
+  const S* zp;
+};
+template <typename S>
+__device__ __forceinline__ Rows<S> rows_at(const S* base, uint32_t e0, const Geom& g, int pitch) {
+  const long long slab = (long long)g.ny * kQ * pitch;
+  return {base + e0, base + e0 - slab, base + e0 + slab};
+}
+// source of direction I (pull), at a compile-time offset from one of the three row pointers when kT > 0
+template <int I, int kT, typename S>
+__device__ __forceinline__ const S* pull_src(const Rows<S>& v, const Geom& g) {
+  const int T = row_len<kT>(g);
+  const S* b = ez_of(I) > 0 ? v.zm : (ez_of(I) < 0 ? v.zp : v.c);
+  return b + (I * T - ex_of(I) - ey_of(I) * kQ * T);
+}
 
 #define XAC_FOR19(M) M(0) M(1) M(2) M(3) M(4) M(5) M(6) M(7) M(8) M(9) M(10) M(11) M(12) M(13) M(14) M(15) M(16) M(17) M(18)
 
-// Lanes sharing one 32-byte DRAM sector of a population plane (planes are 256-byte aligned).
+// Lanes sharing one 32-byte DRAM sector of a population row (rows start on 32-value boundaries).
 template <typename S>
 __device__ __forceinline__ unsigned sector_group(int lane) {
   return sizeof(S) == 4 ? (0xFFu << (lane & ~7)) : (0xFFFFu << (lane & ~15));
@@ -115,24 +148,24 @@ __device__ __forceinline__ unsigned sector_group(int lane) {
 // fluid work: their fluid populations are the rest equilibrium w_i for ever (fluid_engine3d.py:193-194 never
 // streams them, and they start at rho=1, u=0); a solid lane still stores w_i when a fluid lane shares its
 // sector, so every sector of the fluid output is written whole.
-// Population (direction i, cell c) is element c + plane[i] of its array; a pulled source is c + pull[i]. Both
-// indices are formed in 32 bits (every one is non-negative and below 19 N) so each access costs one integer add
-// and one widening multiply-add off the array base.
+// c is the compact cell index (link word, heat source, fields); P/Q are the cell's row pointers into the input
+// populations and Po/Qo its own position in the outputs. Direction i of the cell is at +i*pitch.
 
 // fluid lattice of a non-solid cell: pull with the boundary rules, moments, BGK collision; returns u
-template <typename S, bool kMacro, bool kCoherent = false>
-__device__ __forceinline__ void fluid_cell(const uint32_t c, const S* __restrict__ Pin, S* __restrict__ Pout,
+template <typename S, bool kMacro, bool kCoherent, int kT>
+__device__ __forceinline__ void fluid_cell(const uint32_t c, const Rows<S>& P, S* __restrict__ Po,
                                            const float* __restrict__ u_in_ptr, float* __restrict__ rho_o,
                                            float* __restrict__ ux_o, float* __restrict__ uy_o,
                                            float* __restrict__ uz_o, const StepParams& p, const uint32_t lw,
                                            float& ux, float& uy, float& uz) {
   const int type = link_type(lw);
-  const S* __restrict__ Pc = Pin + c;  // outlet cells copy from Pc - 1
+  const int RL = row_len<kT>(p.g);
+  const S* __restrict__ Pc = P.c;  // outlet cells copy from Pc - 1
   float F[kQ];
   if (type == kInlet) {
     // src/fluid_engine3d.py:197-244: no pull; unknown populations from the known ones
     float k[kQ];
-#define XAC_LD_OWN(I) k[I] = Pop<S>::template ld<kCoherent>(Pin + (c + p.plane[I]), w_of(I));
+#define XAC_LD_OWN(I) k[I] = Pop<S>::template ld<kCoherent>(P.c + (I) * RL, w_of(I));
     XAC_FOR19(XAC_LD_OWN)
 #undef XAC_LD_OWN
     const float ux_in = __ldg(u_in_ptr);
@@ -164,7 +197,7 @@ __device__ __forceinline__ void fluid_cell(const uint32_t c, const S* __restrict
     const S* __restrict__ Ps = (lw & kXLoBit) ? Pc : Pc - 1;
     float sum = 0.0f;
 #define XAC_LD_OUT(I)                              \
-F[I] = Pop<S>::template ld<kCoherent>(Ps + p.plane[I], w_of(I));     \
+F[I] = Pop<S>::template ld<kCoherent>(Ps + (I) * RL, w_of(I));     \
 sum += F[I];
     XAC_FOR19(XAC_LD_OUT)
 #undef XAC_LD_OUT
@@ -176,7 +209,7 @@ sum += F[I];
   } else {
     // src/fluid_engine3d.py:262-272: pull, halfway bounce-back on out-of-domain or solid sources
 #define XAC_LD_PULL(I)                                                                                      \
-F[I] = ((lw >> I) & 1u) ? Pop<S>::template ld<kCoherent>(Pin + (c + p.plane[opp_of(I)]), w_of(I)) : Pop<S>::template ld<kCoherent>(Pin + (c + p.pull[I]), w_of(I));
+F[I] = ((lw >> I) & 1u) ? Pop<S>::template ld<kCoherent>(P.c + (opp_of(I)) * RL, w_of(I)) : Pop<S>::template ld<kCoherent>(pull_src<I, kT>(P, p.g), w_of(I));
     XAC_FOR19(XAC_LD_PULL)
 #undef XAC_LD_PULL
   }
@@ -206,24 +239,25 @@ F[I] = ((lw >> I) & 1u) ? Pop<S>::template ld<kCoherent>(Pin + (c + p.plane[opp_
 #define XAC_COLLIDE(I)                                                            \
 {                                                                               \
   const float fe = feq_term(w_of(I) * r, edotu<I>(ux, uy, uz), usq15);         \
-  Pop<S>::st(Pout + (c + p.plane[I]), F[I] - omega * (F[I] - fe), w_of(I));             \
+  Pop<S>::st(Po + (I) * RL, F[I] - omega * (F[I] - fe), w_of(I));             \
 }
   XAC_FOR19(XAC_COLLIDE)
 #undef XAC_COLLIDE
 }
 
 // fluid lattice of a solid cell: moments of the frozen populations on macro steps, w_i fill of shared sectors
-template <typename S, bool kMacro, bool kCoherent = false>
-__device__ __forceinline__ void solid_cell(const uint32_t c, const S* __restrict__ Pin, S* __restrict__ Pout,
+template <typename S, bool kMacro, bool kCoherent, int kT>
+__device__ __forceinline__ void solid_cell(const uint32_t c, const Rows<S>& P, S* __restrict__ Po,
                                            float* __restrict__ rho_o, float* __restrict__ ux_o,
                                            float* __restrict__ uy_o, float* __restrict__ uz_o,
                                            const StepParams& p, const bool fill_solid) {
+  const int RL = row_len<kT>(p.g);
   if (kMacro) {
     // moments of the frozen solid populations, as the reference's macroscopic kernel computes them
     float r = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f;
 #pragma unroll
     for (int i = 0; i < kQ; ++i) {
-      const float v = Pop<S>::template ld<kCoherent>(Pin + (c + p.plane[i]), w_of(i));
+      const float v = Pop<S>::template ld<kCoherent>(P.c + (i) * RL, w_of(i));
       r += v;
       if (ex_of(i) != 0) mx += ex_of(i) > 0 ? v : -v;
       if (ey_of(i) != 0) my += ey_of(i) > 0 ? v : -v;
@@ -236,23 +270,24 @@ __device__ __forceinline__ void solid_cell(const uint32_t c, const S* __restrict
   }
   if (fill_solid) {
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) Pop<S>::st(Pout + (c + p.plane[i]), w_of(i), w_of(i));
+    for (int i = 0; i < kQ; ++i) Pop<S>::st(Po + (i) * RL, w_of(i), w_of(i));
   }
 }
 
 // thermal lattice of any cell, with the cell's fluid velocity u (0 in solids)
-template <typename S, bool kOwn, bool kCoherent = false>
-__device__ __forceinline__ void thermal_cell(const uint32_t c, const S* __restrict__ Qin, S* __restrict__ Qout,
+template <typename S, bool kOwn, bool kCoherent, int kT>
+__device__ __forceinline__ void thermal_cell(const uint32_t c, const Rows<S>& Q, S* __restrict__ Qo,
                                              const float* __restrict__ qsrc, const float* __restrict__ T0,
                                              const StepParams& p, const uint32_t lw, const float ux, const float uy,
                                              const float uz) {
   const int type = link_type(lw);
-  const S* __restrict__ Qc = Qin + c;  // outlet cells copy from Qc - 1
+  const int RL = row_len<kT>(p.g);
+  const S* __restrict__ Qc = Q.c;  // outlet cells copy from Qc - 1
   const float Tb = p.T_ref;
   float G[kQ];
   float T;
   if (kOwn) {
-#define XAC_LD_G0(I) G[I] = Pop<S>::template ld<kCoherent>(Qin + (c + p.plane[I]), w_of(I) * Tb);
+#define XAC_LD_G0(I) G[I] = Pop<S>::template ld<kCoherent>(Q.c + (I) * RL, w_of(I) * Tb);
     XAC_FOR19(XAC_LD_G0)
 #undef XAC_LD_G0
     T = kCoherent ? __ldcg(T0 + c) : __ldg(T0 + c);
@@ -264,7 +299,7 @@ __device__ __forceinline__ void thermal_cell(const uint32_t c, const S* __restri
     } else if (type == kOutlet) {
       // src/thermal_engine3d.py:170-177
       const S* __restrict__ Qs = (lw & kXLoBit) ? Qc : Qc - 1;
-#define XAC_LD_GOUT(I) G[I] = Pop<S>::template ld<kCoherent>(Qs + p.plane[I], w_of(I) * Tb);
+#define XAC_LD_GOUT(I) G[I] = Pop<S>::template ld<kCoherent>(Qs + (I) * RL, w_of(I) * Tb);
       XAC_FOR19(XAC_LD_GOUT)
 #undef XAC_LD_GOUT
     } else if (!(lw & kYZBit)) {
@@ -273,11 +308,11 @@ __device__ __forceinline__ void thermal_cell(const uint32_t c, const S* __restri
 #define XAC_LD_GFAST(I)                                                                                        \
   {                                                                                                            \
     if (ex_of(I) == 1)                                                                                         \
-      G[I] = (lw & kXLoBit) ? w_of(I) * p.T_in : Pop<S>::template ld<kCoherent>(Qin + (c + p.pull[I]), w_of(I) * Tb);                     \
+      G[I] = (lw & kXLoBit) ? w_of(I) * p.T_in : Pop<S>::template ld<kCoherent>(pull_src<I, kT>(Q, p.g), w_of(I) * Tb);                     \
     else if (ex_of(I) == -1)                                                                                   \
-      G[I] = (lw & kXHiBit) ? Pop<S>::template ld<kCoherent>(Qin + (c + p.plane[I]), w_of(I) * Tb) : Pop<S>::template ld<kCoherent>(Qin + (c + p.pull[I]), w_of(I) * Tb); \
+      G[I] = (lw & kXHiBit) ? Pop<S>::template ld<kCoherent>(Q.c + (I) * RL, w_of(I) * Tb) : Pop<S>::template ld<kCoherent>(pull_src<I, kT>(Q, p.g), w_of(I) * Tb); \
     else                                                                                                       \
-      G[I] = Pop<S>::template ld<kCoherent>(Qin + (c + p.pull[I]), w_of(I) * Tb);                                                         \
+      G[I] = Pop<S>::template ld<kCoherent>(pull_src<I, kT>(Q, p.g), w_of(I) * Tb);                                                         \
   }
       XAC_FOR19(XAC_LD_GFAST)
 #undef XAC_LD_GFAST
@@ -291,11 +326,11 @@ __device__ __forceinline__ void thermal_cell(const uint32_t c, const S* __restri
     if (xlo)                                                                                                   \
       G[I] = w_of(I) * p.T_in;                                                                                 \
     else if (xhi)                                                                                              \
-      G[I] = Pop<S>::template ld<kCoherent>(Qin + (c + p.plane[I]), w_of(I) * Tb);                                                        \
+      G[I] = Pop<S>::template ld<kCoherent>(Q.c + (I) * RL, w_of(I) * Tb);                                                        \
     else if (wall)                                                                                             \
-      G[I] = Pop<S>::template ld<kCoherent>(Qin + (c + p.plane[opp_of(I)]), w_of(I) * Tb);                                                \
+      G[I] = Pop<S>::template ld<kCoherent>(Q.c + (opp_of(I)) * RL, w_of(I) * Tb);                                                \
     else                                                                                                       \
-      G[I] = Pop<S>::template ld<kCoherent>(Qin + (c + p.pull[I]), w_of(I) * Tb);                                                         \
+      G[I] = Pop<S>::template ld<kCoherent>(pull_src<I, kT>(Q, p.g), w_of(I) * Tb);                                                         \
   }
       XAC_FOR19(XAC_LD_GSLOW)
 #undef XAC_LD_GSLOW
@@ -316,33 +351,56 @@ __device__ __forceinline__ void thermal_cell(const uint32_t c, const S* __restri
     const float ge = feq_term(w_of(I) * T, edotu<I>(ux, uy, uz), usq15t);       \
     float v = G[I] - omega_t * (G[I] - ge);                                      \
     if (q > 0.0f) v += (w_of(I) * srcf) * q;                                     \
-    Pop<S>::st(Qout + (c + p.plane[I]), v, w_of(I) * Tb);                                \
+    Pop<S>::st(Qo + (I) * RL, v, w_of(I) * Tb);                                \
   }
   XAC_FOR19(XAC_TCOLLIDE)
 #undef XAC_TCOLLIDE
 }
 
-template <typename S, bool kMacro, bool kOwn, bool kCoherent = false>
-__device__ __forceinline__ void coupled_cell(const uint32_t c, const S* __restrict__ Pin, S* __restrict__ Pout,
-                                             const S* __restrict__ Qin, S* __restrict__ Qout,
-                                             const uint32_t* __restrict__ link, const float* __restrict__ qsrc,
-                                             const float* __restrict__ u_in_ptr, float* __restrict__ rho_o,
-                                             float* __restrict__ ux_o, float* __restrict__ uy_o,
-                                             float* __restrict__ uz_o, const float* __restrict__ T0,
-                                             const StepParams& p, const bool valid, const uint32_t lw,
-                                             const bool fill_solid) {
+// cell c (compact index) whose populations start at element e0 of each array
+template <typename S, bool kMacro, bool kOwn, bool kCoherent, int kT>
+__device__ __forceinline__ void coupled_cell(const uint32_t c, const uint32_t e0, const S* __restrict__ Pin,
+                                             S* __restrict__ Pout, const S* __restrict__ Qin, S* __restrict__ Qout,
+                                             const float* __restrict__ qsrc, const float* __restrict__ u_in_ptr,
+                                             float* __restrict__ rho_o, float* __restrict__ ux_o,
+                                             float* __restrict__ uy_o, float* __restrict__ uz_o,
+                                             const float* __restrict__ T0, const StepParams& p, const bool valid,
+                                             const uint32_t lw, const bool fill_solid) {
+  const int RL = row_len<kT>(p.g);
   const bool fluid = valid && link_type(lw) != kSolid;
   float ux = 0.0f, uy = 0.0f, uz = 0.0f;
   if (fluid)
-    fluid_cell<S, kMacro, kCoherent>(c, Pin, Pout, u_in_ptr, rho_o, ux_o, uy_o, uz_o, p, lw, ux, uy, uz);
+    fluid_cell<S, kMacro, kCoherent, kT>(c, rows_at(Pin, e0, p.g, RL), Pout + e0, u_in_ptr, rho_o, ux_o, uy_o, uz_o,
+                                         p, lw, ux, uy, uz);
   else if (valid)
-    solid_cell<S, kMacro, kCoherent>(c, Pin, Pout, rho_o, ux_o, uy_o, uz_o, p, fill_solid);
+    solid_cell<S, kMacro, kCoherent, kT>(c, rows_at(Pin, e0, p.g, RL), Pout + e0, rho_o, ux_o, uy_o, uz_o, p,
+                                         fill_solid);
   if (!valid) return;
-  thermal_cell<S, kOwn, kCoherent>(c, Qin, Qout, qsrc, T0, p, lw, ux, uy, uz);
+  thermal_cell<S, kOwn, kCoherent, kT>(c, rows_at(Qin, e0, p.g, RL), Qout + e0, qsrc, T0, p, lw, ux, uy, uz);
 }
 
-// kCells cells per thread, at a stride of one block, so each load instruction stays coalesced.
-template <typename S, bool kMacro, bool kOwn, int kCells>
+// Padding positions (x >= nx) of a row's last, partly valid sector store a value too, so that the sector is
+// written whole (no read-modify-write in L2); the values are never read.
+template <typename S, int kT>
+__device__ __forceinline__ void pad_fill(bool valid, unsigned fluid_lanes, unsigned valid_lanes, int lane,
+                                         S* __restrict__ Pout, S* __restrict__ Qout, uint32_t e0, const Geom& g) {
+  if (valid) return;
+  const int RL = row_len<kT>(g);
+  const unsigned grp = sector_group<S>(lane);
+  if (fluid_lanes & grp) {
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) Pop<S>::st(Pout + e0 + i * RL, w_of(i), w_of(i));
+  }
+  if (valid_lanes & grp) {
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) Pop<S>::st(Qout + e0 + i * RL, 0.0f, 0.0f);
+  }
+}
+
+// One thread per row position: block-consecutive threads walk x along a row (a warp never spans two rows, the
+// row length being a multiple of 32); positions x >= nx are padding. kT > 0 makes the row length and every
+// population offset compile-time constants; kT = 0 reads it from the geometry.
+template <typename S, bool kMacro, bool kOwn, int kT>
 __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__ Pin, S* __restrict__ Pout,
                                                            const S* __restrict__ Qin, S* __restrict__ Qout,
                                                            const uint32_t* __restrict__ link,
@@ -351,246 +409,41 @@ __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__
                                                            float* __restrict__ rho_o, float* __restrict__ ux_o,
                                                            float* __restrict__ uy_o, float* __restrict__ uz_o,
                                                            const float* __restrict__ T0, StepParams p) {
-  const uint32_t base = blockIdx.x * blockDim.x * kCells + threadIdx.x;
+  const int RL = row_len<kT>(p.g);
+  const uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t r = pos / (uint32_t)RL, x = pos - r * (uint32_t)RL;
+  if (r >= (uint32_t)p.g.rows) return;  // whole warps
   const int lane = threadIdx.x & 31;
-#pragma unroll
-  for (int j = 0; j < kCells; ++j) {
-    const uint32_t c = base + j * blockDim.x;
-    const bool valid = c < (uint32_t)p.g.ncell;
-    const uint32_t lw = valid ? __ldg(link + c) : ((uint32_t)kSolid << kTypeShift);
-    const unsigned fluid_lanes = __ballot_sync(0xffffffffu, valid && link_type(lw) != kSolid);
-    coupled_cell<S, kMacro, kOwn>(c, Pin, Pout, Qin, Qout, link, qsrc, u_in_ptr, rho_o, ux_o, uy_o, uz_o, T0, p,
-                                  valid, lw, (fluid_lanes & sector_group<S>(lane)) != 0u);
-  }
+  const bool valid = x < (uint32_t)p.g.nx;
+  const uint32_t c = r * (uint32_t)p.g.nx + x;
+  const uint32_t lw = valid ? __ldg(link + c) : ((uint32_t)kSolid << kTypeShift);
+  const unsigned fluid_lanes = __ballot_sync(0xffffffffu, valid && link_type(lw) != kSolid);
+  coupled_cell<S, kMacro, kOwn, false, kT>(c, pop_base(r, x, p.g, RL), Pin, Pout, Qin, Qout, qsrc, u_in_ptr, rho_o,
+                                           ux_o, uy_o, uz_o, T0, p, valid, lw,
+                                           (fluid_lanes & sector_group<S>(lane)) != 0u);
+  pad_fill<S, kT>(valid, fluid_lanes, __ballot_sync(0xffffffffu, valid), lane, Pout, Qout, pop_base(r, x, p.g, RL),
+                  p.g);
 }
 
-// ---- pair-compacted step ------------------------------------------------------------------------
-// A warp owns 64 consecutive cells, two groups of 32. When the two groups hold at most 32 non-solid cells
-// between them (the usual case in a porous design), the fluid lattice of all of them runs in ONE pass over a
-// compacted list - lane l takes the l-th non-solid cell - instead of two passes with the solid lanes idle. Each
-// lane then gets its own cells' velocities back by shuffles and runs the thermal lattice of its two cells.
-// Every cell runs exactly the arithmetic of coupled_cell, so results are identical.
-template <typename S, bool kMacro, bool kOwn>
-__global__ void __launch_bounds__(256) coupled_pair_kernel(const S* __restrict__ Pin, S* __restrict__ Pout,
-                                                           const S* __restrict__ Qin, S* __restrict__ Qout,
-                                                           const uint32_t* __restrict__ link,
-                                                           const float* __restrict__ qsrc,
-                                                           const float* __restrict__ u_in_ptr,
-                                                           float* __restrict__ rho_o, float* __restrict__ ux_o,
-                                                           float* __restrict__ uy_o, float* __restrict__ uz_o,
-                                                           const float* __restrict__ T0, StepParams p) {
-  __shared__ uint8_t slot[8][32];  // per warp: lane l of the compacted pass works on cell base + slot[l]
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t base = (blockIdx.x * (blockDim.x >> 5) + warp) * 64u;
-  const uint32_t ncell = (uint32_t)p.g.ncell;
-  const uint32_t c0 = base + lane, c1 = base + 32u + lane;
-  const bool v0 = c0 < ncell, v1 = c1 < ncell;
-  const uint32_t solid_word = (uint32_t)kSolid << kTypeShift;
-  const uint32_t lw0 = v0 ? __ldg(link + c0) : solid_word, lw1 = v1 ? __ldg(link + c1) : solid_word;
-  const bool f0 = v0 && link_type(lw0) != kSolid, f1 = v1 && link_type(lw1) != kSolid;
-  const unsigned m0 = __ballot_sync(0xffffffffu, f0), m1 = __ballot_sync(0xffffffffu, f1);
-  const int k0 = __popc(m0), k1 = __popc(m1);
-  float ux0 = 0.0f, uy0 = 0.0f, uz0 = 0.0f, ux1 = 0.0f, uy1 = 0.0f, uz1 = 0.0f;
-  if (k0 + k1 <= 32) {
-    const unsigned below = (1u << lane) - 1u;
-    const int r0 = __popc(m0 & below), r1 = k0 + __popc(m1 & below);
-    if (f0) slot[warp][r0] = (uint8_t)lane;
-    if (f1) slot[warp][r1] = (uint8_t)(32 + lane);
-    __syncwarp();
-    const bool work = lane < k0 + k1;
-    const int src = work ? slot[warp][lane] : 0;
-    const uint32_t a = __shfl_sync(0xffffffffu, lw0, src & 31), b = __shfl_sync(0xffffffffu, lw1, src & 31);
-    float ux = 0.0f, uy = 0.0f, uz = 0.0f;
-    if (work)
-      fluid_cell<S, kMacro>(base + (uint32_t)src, Pin, Pout, u_in_ptr, rho_o, ux_o, uy_o, uz_o, p, src < 32 ? a : b,
-                            ux, uy, uz);
-    const float a0 = __shfl_sync(0xffffffffu, ux, r0 & 31), a1 = __shfl_sync(0xffffffffu, uy, r0 & 31),
-                a2 = __shfl_sync(0xffffffffu, uz, r0 & 31);
-    const float b0 = __shfl_sync(0xffffffffu, ux, r1 & 31), b1 = __shfl_sync(0xffffffffu, uy, r1 & 31),
-                b2 = __shfl_sync(0xffffffffu, uz, r1 & 31);
-    if (f0) {
-      ux0 = a0;
-      uy0 = a1;
-      uz0 = a2;
-    }
-    if (f1) {
-      ux1 = b0;
-      uy1 = b1;
-      uz1 = b2;
-    }
-    __syncwarp();
-  } else {
-    if (f0) fluid_cell<S, kMacro>(c0, Pin, Pout, u_in_ptr, rho_o, ux_o, uy_o, uz_o, p, lw0, ux0, uy0, uz0);
-    if (f1) fluid_cell<S, kMacro>(c1, Pin, Pout, u_in_ptr, rho_o, ux_o, uy_o, uz_o, p, lw1, ux1, uy1, uz1);
-  }
-  const unsigned sg = sector_group<S>(lane);
-  if (v0 && !f0) solid_cell<S, kMacro>(c0, Pin, Pout, rho_o, ux_o, uy_o, uz_o, p, (m0 & sg) != 0u);
-  if (v1 && !f1) solid_cell<S, kMacro>(c1, Pin, Pout, rho_o, ux_o, uy_o, uz_o, p, (m1 & sg) != 0u);
-  if (v0) thermal_cell<S, kOwn>(c0, Qin, Qout, qsrc, T0, p, lw0, ux0, uy0, uz0);
-  if (v1) thermal_cell<S, kOwn>(c1, Qin, Qout, qsrc, T0, p, lw1, ux1, uy1, uz1);
-}
-
-// ---- class-grouped step -------------------------------------------------------------------------
-// Cells are visited through an index list grouped by class, so a warp never mixes them:
-//   bulk fluid : fluid label, not on a y/z face  -> both lattices, plain pull, no boundary branches
-//   bulk solid : solid label, not on a y/z face  -> thermal lattice only, with u = 0, where the second-order
-//                equilibrium w_i T (1 + 3e.u + 4.5(e.u)^2 - 1.5u^2) evaluates to exactly w_i T
-//   other      : inlet, outlet and y/z-face cells -> the general per-cell path
-// Every cell runs exactly the arithmetic of coupled_cell, so results are identical.
-enum CellClass : int { kClassBulkFluid = 0, kClassBulkSolid = 1, kClassOther = 2 };
-constexpr uint32_t kNoCell = 0xFFFFFFFFu;
-
-template <typename S, bool kOwn>
-__device__ __forceinline__ void thermal_bulk_pull(const S* __restrict__ Qc, const uint32_t lw, const StepParams& p,
-                                                  const float* __restrict__ T0, const uint32_t c, float (&G)[kQ],
-                                                  float& T) {
-  const float Tb = p.T_ref;
-  if (kOwn) {
-#define XAC_LD_G0(I) G[I] = Pop<S>::ld(Qc + p.plane[I], w_of(I) * Tb);
-    XAC_FOR19(XAC_LD_G0)
-#undef XAC_LD_G0
-    T = __ldg(T0 + c);
-    return;
-  }
-#define XAC_LD_GFAST(I)                                                                                        \
-  {                                                                                                            \
-    if (ex_of(I) == 1)                                                                                         \
-      G[I] = (lw & kXLoBit) ? w_of(I) * p.T_in : Pop<S>::ld(Qc + p.pull[I], w_of(I) * Tb);                     \
-    else if (ex_of(I) == -1)                                                                                   \
-      G[I] = (lw & kXHiBit) ? Pop<S>::ld(Qc + p.plane[I], w_of(I) * Tb) : Pop<S>::ld(Qc + p.pull[I], w_of(I) * Tb); \
-    else                                                                                                       \
-      G[I] = Pop<S>::ld(Qc + p.pull[I], w_of(I) * Tb);                                                         \
-  }
-  XAC_FOR19(XAC_LD_GFAST)
-#undef XAC_LD_GFAST
-  T = 0.0f;
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) T += G[i];
-}
-
-template <typename S, bool kMacro, bool kOwn>
-__device__ __forceinline__ void bulk_fluid_cell(const uint32_t c, const uint32_t lw, const S* __restrict__ Pin,
-                                                S* __restrict__ Pout, const S* __restrict__ Qin,
-                                                S* __restrict__ Qout, const float* __restrict__ qsrc,
-                                                float* __restrict__ rho_o, float* __restrict__ ux_o,
-                                                float* __restrict__ uy_o, float* __restrict__ uz_o,
-                                                const float* __restrict__ T0, const StepParams& p) {
-  const S* __restrict__ Pc = Pin + c;
-  S* __restrict__ Po = Pout + c;
-  float F[kQ];
-#define XAC_LD_PULL(I)                                                                                      \
-  F[I] = ((lw >> I) & 1u) ? Pop<S>::ld(Pc + p.plane[opp_of(I)], w_of(I)) : Pop<S>::ld(Pc + p.pull[I], w_of(I));
-  XAC_FOR19(XAC_LD_PULL)
-#undef XAC_LD_PULL
-  float r = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f;
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) {
-    r += F[i];
-    if (ex_of(i) != 0) mx += ex_of(i) > 0 ? F[i] : -F[i];
-    if (ey_of(i) != 0) my += ey_of(i) > 0 ? F[i] : -F[i];
-    if (ez_of(i) != 0) mz += ez_of(i) > 0 ? F[i] : -F[i];
-  }
-  float ux = 0.0f, uy = 0.0f, uz = 0.0f;
-  if (r > 1e-10f) {
-    ux = mx / r;
-    uy = my / r;
-    uz = mz / r;
-  }
-  if (kMacro) {
-    rho_o[c] = r;
-    ux_o[c] = ux;
-    uy_o[c] = uy;
-    uz_o[c] = uz;
-  }
-  const float omega = p.omega_f;
-  const float usq15 = 1.5f * ((ux * ux + uy * uy) + uz * uz);
-#define XAC_COLLIDE(I)                                                            \
-  {                                                                               \
-    const float fe = feq_term(w_of(I) * r, edotu<I>(ux, uy, uz), usq15);         \
-    Pop<S>::st(Po + p.plane[I], F[I] - omega * (F[I] - fe), w_of(I));             \
-  }
-  XAC_FOR19(XAC_COLLIDE)
-#undef XAC_COLLIDE
-  float G[kQ], T;
-  thermal_bulk_pull<S, kOwn>(Qin + c, lw, p, T0, c, G, T);
-  S* __restrict__ Qo = Qout + c;
-  const float omega_t = p.omega_tf, srcf = p.srcf_f;
-  const float q = (lw & kHeatedBit) ? __ldg(qsrc + c) : 0.0f;
-  const float usq15t = 1.5f * ((ux * ux + uy * uy) + uz * uz);
-  const float Tb = p.T_ref;
-#define XAC_TCOLLIDE(I)                                                          \
-  {                                                                              \
-    const float ge = feq_term(w_of(I) * T, edotu<I>(ux, uy, uz), usq15t);       \
-    float v = G[I] - omega_t * (G[I] - ge);                                      \
-    if (q > 0.0f) v += (w_of(I) * srcf) * q;                                     \
-    Pop<S>::st(Qo + p.plane[I], v, w_of(I) * Tb);                                \
-  }
-  XAC_FOR19(XAC_TCOLLIDE)
-#undef XAC_TCOLLIDE
-}
-
-template <typename S, bool kMacro, bool kOwn>
-__device__ __forceinline__ void bulk_solid_cell(const uint32_t c, const uint32_t lw, S* __restrict__ Pout,
-                                                const S* __restrict__ Qin, S* __restrict__ Qout,
-                                                const float* __restrict__ qsrc, float* __restrict__ rho_o,
-                                                float* __restrict__ ux_o, float* __restrict__ uy_o,
-                                                float* __restrict__ uz_o, const float* __restrict__ T0,
-                                                const StepParams& p) {
-  if (kMacro) {
-    // the frozen solid populations are w_i: rho = sum of w_i in order, u = 0
-    float r = 0.0f;
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) r += w_of(i);
-    rho_o[c] = r;
-    ux_o[c] = 0.0f;
-    uy_o[c] = 0.0f;
-    uz_o[c] = 0.0f;
-  }
-  if (lw & kFillBit) {
-    S* __restrict__ Po = Pout + c;
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) Pop<S>::st(Po + p.plane[i], w_of(i), w_of(i));
-  }
-  float G[kQ], T;
-  thermal_bulk_pull<S, kOwn>(Qin + c, lw, p, T0, c, G, T);
-  S* __restrict__ Qo = Qout + c;
-  const float omega_t = p.omega_ts, srcf = p.srcf_s;
-  const float q = (lw & kHeatedBit) ? __ldg(qsrc + c) : 0.0f;
-  const float Tb = p.T_ref;
-#define XAC_TCOLLIDE_S(I)                                                        \
-  {                                                                              \
-    const float ge = w_of(I) * T;                                                \
-    float v = G[I] - omega_t * (G[I] - ge);                                      \
-    if (q > 0.0f) v += (w_of(I) * srcf) * q;                                     \
-    Pop<S>::st(Qo + p.plane[I], v, w_of(I) * Tb);                                \
-  }
-  XAC_FOR19(XAC_TCOLLIDE_S)
-#undef XAC_TCOLLIDE_S
-}
-
-// cells: the three class lists concatenated, each padded with kNoCell to a multiple of 512 so that every
-// block (<= 512 threads, a divisor of 512) sees one class. class_end: end of each class in the list.
-template <typename S, bool kMacro, bool kOwn>
-__global__ void __launch_bounds__(256) coupled_step_grouped_kernel(
-    const uint32_t* __restrict__ cells, uint32_t end_fluid, uint32_t end_solid, const S* __restrict__ Pin,
-    S* __restrict__ Pout, const S* __restrict__ Qin, S* __restrict__ Qout, const uint32_t* __restrict__ link,
-    const float* __restrict__ qsrc, const float* __restrict__ u_in_ptr, float* __restrict__ rho_o,
-    float* __restrict__ ux_o, float* __restrict__ uy_o, float* __restrict__ uz_o, const float* __restrict__ T0,
-    StepParams p) {
-  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t c = __ldg(cells + idx);
-  if (c == kNoCell) return;
-  const uint32_t lw = __ldg(link + c);
-  const uint32_t first = blockIdx.x * blockDim.x;
-  if (first < end_fluid) {
-    bulk_fluid_cell<S, kMacro, kOwn>(c, lw, Pin, Pout, Qin, Qout, qsrc, rho_o, ux_o, uy_o, uz_o, T0, p);
-  } else if (first < end_solid) {
-    bulk_solid_cell<S, kMacro, kOwn>(c, lw, Pout, Qin, Qout, qsrc, rho_o, ux_o, uy_o, uz_o, T0, p);
-  } else {
-    coupled_cell<S, kMacro, kOwn>(c, Pin, Pout, Qin, Qout, link, qsrc, u_in_ptr, rho_o, ux_o, uy_o, uz_o, T0, p,
-                                  true, lw, (lw & kFillBit) != 0u);
-  }
-}
+// Arguments of one fused step launch; launch_coupled_step<S> (step_kernels.cuh, one translation unit per storage
+// type) picks the instantiation whose compile-time row length matches the lattice.
+struct StepLaunch {
+  const void* Pin;
+  void* Pout;
+  const void* Qin;
+  void* Qout;
+  const uint32_t* link;
+  const float* qsrc;
+  const float* u_in;
+  float *rho, *ux, *uy, *uz;
+  const float* T0;
+  StepParams p;
+  int block;
+  bool macro, own;
+  cudaStream_t stream;
+};
+template <typename S>
+void launch_coupled_step(const StepLaunch& a);
 
 // omega and source factors, computed with the device's IEEE division once per lattice
 static __global__ void relaxation_factors_kernel(float tau_f, float tau_tf, float tau_ts, float* out) {
@@ -602,17 +455,18 @@ static __global__ void relaxation_factors_kernel(float tau_f, float tau_tf, floa
   out[4] = 1.0f - 0.5f * ots;
 }
 
-// T^k = sum of the streamed thermal populations, without storing them (stats / field export steps).
-template <typename S>
-__global__ void __launch_bounds__(256) thermal_finalize_kernel(const S* __restrict__ Qin,
-                                                               const uint32_t* __restrict__ link,
-                                                               float* __restrict__ T_o, StepParams p) {
-  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= (uint32_t)p.g.ncell) return;
+// T^k = sum of the streamed thermal populations of compact cell c, without storing them (stats / field export
+// steps and the batch kernel's stats steps).
+template <typename S, bool kCoherent>
+__device__ __forceinline__ float finalize_T_cell(const S* __restrict__ Qin, const uint32_t* __restrict__ link,
+                                                 const StepParams& p, uint32_t c) {
   const uint32_t lw = __ldg(link + c);
   const int type = link_type(lw);
   const float Tb = p.T_ref;
-  const S* __restrict__ Qc = Qin + c;
+  const int RL = p.g.pitch;
+  const uint32_t r = c / (uint32_t)p.g.nx, x = c - r * (uint32_t)p.g.nx;
+  const Rows<S> Q = rows_at(Qin, pop_base(r, x, p.g, RL), p.g, RL);
+  const S* __restrict__ Qc = Q.c;
   float T = 0.0f;
   if (type == kInlet) {
 #pragma unroll
@@ -620,7 +474,7 @@ __global__ void __launch_bounds__(256) thermal_finalize_kernel(const S* __restri
   } else if (type == kOutlet) {
     const S* __restrict__ Qs = (lw & kXLoBit) ? Qc : Qc - 1;
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) T += Pop<S>::ld(Qs + p.plane[i], w_of(i) * Tb);
+    for (int i = 0; i < kQ; ++i) T += Pop<S>::template ld<kCoherent>(Qs + i * RL, w_of(i) * Tb);
   } else {
 #define XAC_T_PULL(I)                                                                                          \
   {                                                                                                            \
@@ -631,17 +485,26 @@ __global__ void __launch_bounds__(256) thermal_finalize_kernel(const S* __restri
     if (xlo)                                                                                                   \
       v = w_of(I) * p.T_in;                                                                                    \
     else if (xhi)                                                                                              \
-      v = Pop<S>::ld(Qc + p.plane[I], w_of(I) * Tb);                                                           \
+      v = Pop<S>::template ld<kCoherent>(Qc + (I) * RL, w_of(I) * Tb);                                         \
     else if (wall)                                                                                             \
-      v = Pop<S>::ld(Qc + p.plane[opp_of(I)], w_of(I) * Tb);                                                   \
+      v = Pop<S>::template ld<kCoherent>(Qc + opp_of(I) * RL, w_of(I) * Tb);                                   \
     else                                                                                                       \
-      v = Pop<S>::ld(Qc + p.pull[I], w_of(I) * Tb);                                                            \
+      v = Pop<S>::template ld<kCoherent>(pull_src<I, 0>(Q, p.g), w_of(I) * Tb);                                \
     T += v;                                                                                                    \
   }
     XAC_FOR19(XAC_T_PULL)
 #undef XAC_T_PULL
   }
-  T_o[c] = T;
+  return T;
+}
+
+template <typename S>
+__global__ void __launch_bounds__(256) thermal_finalize_kernel(const S* __restrict__ Qin,
+                                                               const uint32_t* __restrict__ link,
+                                                               float* __restrict__ T_o, StepParams p) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= (uint32_t)p.g.ncell) return;
+  T_o[c] = finalize_T_cell<S, false>(Qin, link, p, c);
 }
 
 }  // namespace xac
