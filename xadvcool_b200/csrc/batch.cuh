@@ -100,7 +100,7 @@ __device__ __forceinline__ void batch_step_tile(const BatchDesign& d, uint32_t t
   const uint32_t lw = valid ? __ldg(d.link + c) : ((uint32_t)kSolid << kTypeShift);
   const unsigned fluid_lanes = __ballot_sync(0xffffffffu, valid && link_type(lw) != kSolid);
   const int lane = threadIdx.x & 31;
-  coupled_cell<S, kMacro, kOwn, true, 0>(c, pop_base(r, x, d.p.g, (int)pitch), (const S*)d.P[cur], (S*)d.P[cur ^ 1],
+  coupled_cell<S, kMacro, kOwn, 1, 0>(c, pop_base(r, x, d.p.g, (int)pitch), (const S*)d.P[cur], (S*)d.P[cur ^ 1],
                                          (const S*)d.Q[cur], (S*)d.Q[cur ^ 1], d.qsrc, d.u_in, d.rho, d.ux, d.uy,
                                          d.uz, d.T, d.p, valid, lw, (fluid_lanes & sector_group<S>(lane)) != 0u);
   pad_fill<S, 0>(valid, fluid_lanes, __ballot_sync(0xffffffffu, valid), lane, (S*)d.P[cur ^ 1], (S*)d.Q[cur ^ 1],

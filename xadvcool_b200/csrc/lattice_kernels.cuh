@@ -71,31 +71,31 @@ __device__ __forceinline__ uint32_t pop_base(uint32_t r, uint32_t x, const Geom&
 // FP32 stores the population itself. The 16-bit forms store the deviation from the rest
 // equilibrium w_i*ref (ref = 1 for the fluid, T_inlet for the thermal lattice) and do all
 // arithmetic in float32.
-// kCoherent loads go through L2 (ld.global.cg): needed when the data was written earlier in the same launch
-// (the persistent batch kernel); otherwise the read-only path (ld.global.nc) is used.
+// Load modes: 0 = read-only path (ld.global.nc); 1 = through L2 (ld.global.cg), needed when the data was written
+// earlier in the same launch (the persistent batch kernel); 2 = plain load (values staged in shared memory).
 template <typename S>
 struct Pop;
 template <>
 struct Pop<float> {
-  template <bool kCoherent = false>
+  template <int kLd = 0>
   static __device__ __forceinline__ float ld(const float* p, float) {
-    return kCoherent ? __ldcg(p) : __ldg(p);
+    return kLd == 2 ? *p : (kLd == 1 ? __ldcg(p) : __ldg(p));
   }
   static __device__ __forceinline__ void st(float* p, float v, float) { *p = v; }
 };
 template <>
 struct Pop<__half> {
-  template <bool kCoherent = false>
+  template <int kLd = 0>
   static __device__ __forceinline__ float ld(const __half* p, float base) {
-    return __half2float(kCoherent ? __ldcg(p) : __ldg(p)) + base;
+    return __half2float(kLd == 2 ? *p : (kLd == 1 ? __ldcg(p) : __ldg(p))) + base;
   }
   static __device__ __forceinline__ void st(__half* p, float v, float base) { *p = __float2half_rn(v - base); }
 };
 template <>
 struct Pop<__nv_bfloat16> {
-  template <bool kCoherent = false>
+  template <int kLd = 0>
   static __device__ __forceinline__ float ld(const __nv_bfloat16* p, float base) {
-    return __bfloat162float(kCoherent ? __ldcg(p) : __ldg(p)) + base;
+    return __bfloat162float(kLd == 2 ? *p : (kLd == 1 ? __ldcg(p) : __ldg(p))) + base;
   }
   static __device__ __forceinline__ void st(__nv_bfloat16* p, float v, float base) {
     *p = __float2bfloat16_rn(v - base);
@@ -115,25 +115,28 @@ struct StepParams {
   float omega_f, omega_tf, omega_ts, srcf_f, srcf_s;
 };
 
-// One cell's view of a population array: the cell's own position (direction 0) and the same x in the rows one
-// z-slab below (source of directions with ez = +1) and above (ez = -1).
-template <typename S>
+// One cell's view of a population array in global memory: the cell's own position (direction 0) and the same x
+// in the rows one z-slab below (source of directions with ez = +1) and above (ez = -1). own(i) is the cell's
+// direction i, pull<I>() the source of direction I (a compile-time offset from one of the three pointers when
+// kT > 0).
+template <typename S, int kT>
 struct Rows {
   const S* c;
   const S* zm;
   const S* zp;
+  int RL;
+  __device__ __forceinline__ const S* own(int i) const { return c + i * (kT > 0 ? kT : RL); }
+  template <int I>
+  __device__ __forceinline__ const S* pull() const {
+    const int T = kT > 0 ? kT : RL;
+    const S* b = ez_of(I) > 0 ? zm : (ez_of(I) < 0 ? zp : c);
+    return b + (I * T - ex_of(I) - ey_of(I) * kQ * T);
+  }
 };
-template <typename S>
-__device__ __forceinline__ Rows<S> rows_at(const S* base, uint32_t e0, const Geom& g, int pitch) {
+template <int kT, typename S>
+__device__ __forceinline__ Rows<S, kT> rows_at(const S* base, uint32_t e0, const Geom& g, int pitch) {
   const long long slab = (long long)g.ny * kQ * pitch;
-  return {base + e0, base + e0 - slab, base + e0 + slab};
-}
-// source of direction I (pull), at a compile-time offset from one of the three row pointers when kT > 0
-template <int I, int kT, typename S>
-__device__ __forceinline__ const S* pull_src(const Rows<S>& v, const Geom& g) {
-  const int T = row_len<kT>(g);
-  const S* b = ez_of(I) > 0 ? v.zm : (ez_of(I) < 0 ? v.zp : v.c);
-  return b + (I * T - ex_of(I) - ey_of(I) * kQ * T);
+  return {base + e0, base + e0 - slab, base + e0 + slab, pitch};
 }
 
 #define XAC_FOR19(M) M(0) M(1) M(2) M(3) M(4) M(5) M(6) M(7) M(8) M(9) M(10) M(11) M(12) M(13) M(14) M(15) M(16) M(17) M(18)
@@ -152,20 +155,19 @@ __device__ __forceinline__ unsigned sector_group(int lane) {
 // populations and Po/Qo its own position in the outputs. Direction i of the cell is at +i*pitch.
 
 // fluid lattice of a non-solid cell: pull with the boundary rules, moments, BGK collision; returns u
-template <typename S, bool kMacro, bool kCoherent, int kT>
-__device__ __forceinline__ void fluid_cell(const uint32_t c, const Rows<S>& P, S* __restrict__ Po,
+template <typename S, bool kMacro, int kLd, int kT, class Acc>
+__device__ __forceinline__ void fluid_cell(const uint32_t c, const Acc& P, S* __restrict__ Po,
                                            const float* __restrict__ u_in_ptr, float* __restrict__ rho_o,
                                            float* __restrict__ ux_o, float* __restrict__ uy_o,
                                            float* __restrict__ uz_o, const StepParams& p, const uint32_t lw,
                                            float& ux, float& uy, float& uz) {
   const int type = link_type(lw);
   const int RL = row_len<kT>(p.g);
-  const S* __restrict__ Pc = P.c;  // outlet cells copy from Pc - 1
   float F[kQ];
   if (type == kInlet) {
     // src/fluid_engine3d.py:197-244: no pull; unknown populations from the known ones
     float k[kQ];
-#define XAC_LD_OWN(I) k[I] = Pop<S>::template ld<kCoherent>(P.c + (I) * RL, w_of(I));
+#define XAC_LD_OWN(I) k[I] = Pop<S>::template ld<kLd>(P.own(I), w_of(I));
     XAC_FOR19(XAC_LD_OWN)
 #undef XAC_LD_OWN
     const float ux_in = __ldg(u_in_ptr);
@@ -194,10 +196,10 @@ __device__ __forceinline__ void fluid_cell(const uint32_t c, const Rows<S>& P, S
     F[18] = k[18];
   } else if (type == kOutlet) {
     // src/fluid_engine3d.py:247-259: copy post-collision (x-1) and rescale to rho_outlet
-    const S* __restrict__ Ps = (lw & kXLoBit) ? Pc : Pc - 1;
+    const int dxo = (lw & kXLoBit) ? 0 : -1;
     float sum = 0.0f;
 #define XAC_LD_OUT(I)                              \
-F[I] = Pop<S>::template ld<kCoherent>(Ps + (I) * RL, w_of(I));     \
+F[I] = Pop<S>::template ld<kLd>(P.own(I) + dxo, w_of(I));     \
 sum += F[I];
     XAC_FOR19(XAC_LD_OUT)
 #undef XAC_LD_OUT
@@ -209,7 +211,7 @@ sum += F[I];
   } else {
     // src/fluid_engine3d.py:262-272: pull, halfway bounce-back on out-of-domain or solid sources
 #define XAC_LD_PULL(I)                                                                                      \
-F[I] = ((lw >> I) & 1u) ? Pop<S>::template ld<kCoherent>(P.c + (opp_of(I)) * RL, w_of(I)) : Pop<S>::template ld<kCoherent>(pull_src<I, kT>(P, p.g), w_of(I));
+F[I] = ((lw >> I) & 1u) ? Pop<S>::template ld<kLd>(P.own(opp_of(I)), w_of(I)) : Pop<S>::template ld<kLd>(P.template pull<I>(), w_of(I));
     XAC_FOR19(XAC_LD_PULL)
 #undef XAC_LD_PULL
   }
@@ -246,8 +248,8 @@ F[I] = ((lw >> I) & 1u) ? Pop<S>::template ld<kCoherent>(P.c + (opp_of(I)) * RL,
 }
 
 // fluid lattice of a solid cell: moments of the frozen populations on macro steps, w_i fill of shared sectors
-template <typename S, bool kMacro, bool kCoherent, int kT>
-__device__ __forceinline__ void solid_cell(const uint32_t c, const Rows<S>& P, S* __restrict__ Po,
+template <typename S, bool kMacro, int kLd, int kT, class Acc>
+__device__ __forceinline__ void solid_cell(const uint32_t c, const Acc& P, S* __restrict__ Po,
                                            float* __restrict__ rho_o, float* __restrict__ ux_o,
                                            float* __restrict__ uy_o, float* __restrict__ uz_o,
                                            const StepParams& p, const bool fill_solid) {
@@ -257,7 +259,7 @@ __device__ __forceinline__ void solid_cell(const uint32_t c, const Rows<S>& P, S
     float r = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f;
 #pragma unroll
     for (int i = 0; i < kQ; ++i) {
-      const float v = Pop<S>::template ld<kCoherent>(P.c + (i) * RL, w_of(i));
+      const float v = Pop<S>::template ld<kLd>(P.own(i), w_of(i));
       r += v;
       if (ex_of(i) != 0) mx += ex_of(i) > 0 ? v : -v;
       if (ey_of(i) != 0) my += ey_of(i) > 0 ? v : -v;
@@ -275,22 +277,21 @@ __device__ __forceinline__ void solid_cell(const uint32_t c, const Rows<S>& P, S
 }
 
 // thermal lattice of any cell, with the cell's fluid velocity u (0 in solids)
-template <typename S, bool kOwn, bool kCoherent, int kT>
-__device__ __forceinline__ void thermal_cell(const uint32_t c, const Rows<S>& Q, S* __restrict__ Qo,
+template <typename S, bool kOwn, int kLd, int kT, class Acc>
+__device__ __forceinline__ void thermal_cell(const uint32_t c, const Acc& Q, S* __restrict__ Qo,
                                              const float* __restrict__ qsrc, const float* __restrict__ T0,
                                              const StepParams& p, const uint32_t lw, const float ux, const float uy,
                                              const float uz) {
   const int type = link_type(lw);
   const int RL = row_len<kT>(p.g);
-  const S* __restrict__ Qc = Q.c;  // outlet cells copy from Qc - 1
   const float Tb = p.T_ref;
   float G[kQ];
   float T;
   if (kOwn) {
-#define XAC_LD_G0(I) G[I] = Pop<S>::template ld<kCoherent>(Q.c + (I) * RL, w_of(I) * Tb);
+#define XAC_LD_G0(I) G[I] = Pop<S>::template ld<kLd>(Q.own(I), w_of(I) * Tb);
     XAC_FOR19(XAC_LD_G0)
 #undef XAC_LD_G0
-    T = kCoherent ? __ldcg(T0 + c) : __ldg(T0 + c);
+    T = kLd == 1 ? __ldcg(T0 + c) : __ldg(T0 + c);  // T0 lives in global memory
   } else {
     if (type == kInlet) {
       // src/thermal_engine3d.py:160-165
@@ -298,8 +299,8 @@ __device__ __forceinline__ void thermal_cell(const uint32_t c, const Rows<S>& Q,
       for (int i = 0; i < kQ; ++i) G[i] = w_of(i) * p.T_in;
     } else if (type == kOutlet) {
       // src/thermal_engine3d.py:170-177
-      const S* __restrict__ Qs = (lw & kXLoBit) ? Qc : Qc - 1;
-#define XAC_LD_GOUT(I) G[I] = Pop<S>::template ld<kCoherent>(Qs + (I) * RL, w_of(I) * Tb);
+      const int dxo = (lw & kXLoBit) ? 0 : -1;
+#define XAC_LD_GOUT(I) G[I] = Pop<S>::template ld<kLd>(Q.own(I) + dxo, w_of(I) * Tb);
       XAC_FOR19(XAC_LD_GOUT)
 #undef XAC_LD_GOUT
     } else if (!(lw & kYZBit)) {
@@ -308,11 +309,11 @@ __device__ __forceinline__ void thermal_cell(const uint32_t c, const Rows<S>& Q,
 #define XAC_LD_GFAST(I)                                                                                        \
   {                                                                                                            \
     if (ex_of(I) == 1)                                                                                         \
-      G[I] = (lw & kXLoBit) ? w_of(I) * p.T_in : Pop<S>::template ld<kCoherent>(pull_src<I, kT>(Q, p.g), w_of(I) * Tb);                     \
+      G[I] = (lw & kXLoBit) ? w_of(I) * p.T_in : Pop<S>::template ld<kLd>(Q.template pull<I>(), w_of(I) * Tb);                     \
     else if (ex_of(I) == -1)                                                                                   \
-      G[I] = (lw & kXHiBit) ? Pop<S>::template ld<kCoherent>(Q.c + (I) * RL, w_of(I) * Tb) : Pop<S>::template ld<kCoherent>(pull_src<I, kT>(Q, p.g), w_of(I) * Tb); \
+      G[I] = (lw & kXHiBit) ? Pop<S>::template ld<kLd>(Q.own(I), w_of(I) * Tb) : Pop<S>::template ld<kLd>(Q.template pull<I>(), w_of(I) * Tb); \
     else                                                                                                       \
-      G[I] = Pop<S>::template ld<kCoherent>(pull_src<I, kT>(Q, p.g), w_of(I) * Tb);                                                         \
+      G[I] = Pop<S>::template ld<kLd>(Q.template pull<I>(), w_of(I) * Tb);                                                         \
   }
       XAC_FOR19(XAC_LD_GFAST)
 #undef XAC_LD_GFAST
@@ -326,11 +327,11 @@ __device__ __forceinline__ void thermal_cell(const uint32_t c, const Rows<S>& Q,
     if (xlo)                                                                                                   \
       G[I] = w_of(I) * p.T_in;                                                                                 \
     else if (xhi)                                                                                              \
-      G[I] = Pop<S>::template ld<kCoherent>(Q.c + (I) * RL, w_of(I) * Tb);                                                        \
+      G[I] = Pop<S>::template ld<kLd>(Q.own(I), w_of(I) * Tb);                                                        \
     else if (wall)                                                                                             \
-      G[I] = Pop<S>::template ld<kCoherent>(Q.c + (opp_of(I)) * RL, w_of(I) * Tb);                                                \
+      G[I] = Pop<S>::template ld<kLd>(Q.own(opp_of(I)), w_of(I) * Tb);                                                \
     else                                                                                                       \
-      G[I] = Pop<S>::template ld<kCoherent>(pull_src<I, kT>(Q, p.g), w_of(I) * Tb);                                                         \
+      G[I] = Pop<S>::template ld<kLd>(Q.template pull<I>(), w_of(I) * Tb);                                                         \
   }
       XAC_FOR19(XAC_LD_GSLOW)
 #undef XAC_LD_GSLOW
@@ -358,7 +359,7 @@ __device__ __forceinline__ void thermal_cell(const uint32_t c, const Rows<S>& Q,
 }
 
 // cell c (compact index) whose populations start at element e0 of each array
-template <typename S, bool kMacro, bool kOwn, bool kCoherent, int kT>
+template <typename S, bool kMacro, bool kOwn, int kLd, int kT>
 __device__ __forceinline__ void coupled_cell(const uint32_t c, const uint32_t e0, const S* __restrict__ Pin,
                                              S* __restrict__ Pout, const S* __restrict__ Qin, S* __restrict__ Qout,
                                              const float* __restrict__ qsrc, const float* __restrict__ u_in_ptr,
@@ -370,13 +371,13 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const uint32_t e0
   const bool fluid = valid && link_type(lw) != kSolid;
   float ux = 0.0f, uy = 0.0f, uz = 0.0f;
   if (fluid)
-    fluid_cell<S, kMacro, kCoherent, kT>(c, rows_at(Pin, e0, p.g, RL), Pout + e0, u_in_ptr, rho_o, ux_o, uy_o, uz_o,
-                                         p, lw, ux, uy, uz);
+    fluid_cell<S, kMacro, kLd, kT>(c, rows_at<kT>(Pin, e0, p.g, RL), Pout + e0, u_in_ptr, rho_o, ux_o, uy_o, uz_o, p,
+                                   lw, ux, uy, uz);
   else if (valid)
-    solid_cell<S, kMacro, kCoherent, kT>(c, rows_at(Pin, e0, p.g, RL), Pout + e0, rho_o, ux_o, uy_o, uz_o, p,
-                                         fill_solid);
+    solid_cell<S, kMacro, kLd, kT>(c, rows_at<kT>(Pin, e0, p.g, RL), Pout + e0, rho_o, ux_o, uy_o, uz_o, p,
+                                   fill_solid);
   if (!valid) return;
-  thermal_cell<S, kOwn, kCoherent, kT>(c, rows_at(Qin, e0, p.g, RL), Qout + e0, qsrc, T0, p, lw, ux, uy, uz);
+  thermal_cell<S, kOwn, kLd, kT>(c, rows_at<kT>(Qin, e0, p.g, RL), Qout + e0, qsrc, T0, p, lw, ux, uy, uz);
 }
 
 // Padding positions (x >= nx) of a row's last, partly valid sector store a value too, so that the sector is
@@ -418,7 +419,7 @@ __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__
   const uint32_t c = r * (uint32_t)p.g.nx + x;
   const uint32_t lw = valid ? __ldg(link + c) : ((uint32_t)kSolid << kTypeShift);
   const unsigned fluid_lanes = __ballot_sync(0xffffffffu, valid && link_type(lw) != kSolid);
-  coupled_cell<S, kMacro, kOwn, false, kT>(c, pop_base(r, x, p.g, RL), Pin, Pout, Qin, Qout, qsrc, u_in_ptr, rho_o,
+  coupled_cell<S, kMacro, kOwn, 0, kT>(c, pop_base(r, x, p.g, RL), Pin, Pout, Qin, Qout, qsrc, u_in_ptr, rho_o,
                                            ux_o, uy_o, uz_o, T0, p, valid, lw,
                                            (fluid_lanes & sector_group<S>(lane)) != 0u);
   pad_fill<S, kT>(valid, fluid_lanes, __ballot_sync(0xffffffffu, valid), lane, Pout, Qout, pop_base(r, x, p.g, RL),
@@ -465,16 +466,15 @@ __device__ __forceinline__ float finalize_T_cell(const S* __restrict__ Qin, cons
   const float Tb = p.T_ref;
   const int RL = p.g.pitch;
   const uint32_t r = c / (uint32_t)p.g.nx, x = c - r * (uint32_t)p.g.nx;
-  const Rows<S> Q = rows_at(Qin, pop_base(r, x, p.g, RL), p.g, RL);
-  const S* __restrict__ Qc = Q.c;
+  const Rows<S, 0> Q = rows_at<0>(Qin, pop_base(r, x, p.g, RL), p.g, RL);
   float T = 0.0f;
   if (type == kInlet) {
 #pragma unroll
     for (int i = 0; i < kQ; ++i) T += w_of(i) * p.T_in;
   } else if (type == kOutlet) {
-    const S* __restrict__ Qs = (lw & kXLoBit) ? Qc : Qc - 1;
+    const int dxo = (lw & kXLoBit) ? 0 : -1;
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) T += Pop<S>::template ld<kCoherent>(Qs + i * RL, w_of(i) * Tb);
+    for (int i = 0; i < kQ; ++i) T += Pop<S>::template ld<kCoherent>(Q.own(i) + dxo, w_of(i) * Tb);
   } else {
 #define XAC_T_PULL(I)                                                                                          \
   {                                                                                                            \
@@ -485,11 +485,11 @@ __device__ __forceinline__ float finalize_T_cell(const S* __restrict__ Qin, cons
     if (xlo)                                                                                                   \
       v = w_of(I) * p.T_in;                                                                                    \
     else if (xhi)                                                                                              \
-      v = Pop<S>::template ld<kCoherent>(Qc + (I) * RL, w_of(I) * Tb);                                         \
+      v = Pop<S>::template ld<kCoherent>(Q.own(I), w_of(I) * Tb);                                               \
     else if (wall)                                                                                             \
-      v = Pop<S>::template ld<kCoherent>(Qc + opp_of(I) * RL, w_of(I) * Tb);                                   \
+      v = Pop<S>::template ld<kCoherent>(Q.own(opp_of(I)), w_of(I) * Tb);                                     \
     else                                                                                                       \
-      v = Pop<S>::template ld<kCoherent>(pull_src<I, 0>(Q, p.g), w_of(I) * Tb);                                \
+      v = Pop<S>::template ld<kCoherent>(Q.template pull<I>(), w_of(I) * Tb);                                \
     T += v;                                                                                                    \
   }
     XAC_FOR19(XAC_T_PULL)
