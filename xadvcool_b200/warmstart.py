@@ -69,53 +69,130 @@ def generate(seeds, *, max_steps=30000, tol=1e-6, batch_size=64, log=print):
     return torch.cat(feats, 0), torch.cat(tgts, 0), info
 
 
-def train_surrogate(feats, tgts, *, epochs=30, batch=4, lr=5e-4, clip=1.0, val_frac=0.05, seed=0, log=print):
+def _allreduce_(t):
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t)
+    return t
+
+
+def _world():
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized():
+        return dist.get_rank(), dist.get_world_size()
+    return 0, 1
+
+
+def gather_designs(feats, tgts):
+    """Every rank's generated designs to every rank, in rank order (one all-gather of each tensor, padded to the
+    largest shard; the counts are gathered first)."""
+    import torch.distributed as dist
+    rank, world = _world()
+    if world == 1:
+        return feats, tgts
+    n = torch.tensor([feats.shape[0]], device=feats.device)
+    counts = [torch.zeros_like(n) for _ in range(world)]
+    dist.all_gather(counts, n)
+    counts = [int(c) for c in counts]
+    m = max(counts)
+    out = []
+    for t in (feats, tgts):
+        pad = torch.zeros((m,) + tuple(t.shape[1:]), dtype=t.dtype, device=t.device)
+        pad[:t.shape[0]] = t
+        parts = [torch.empty_like(pad) for _ in range(world)]
+        dist.all_gather(parts, pad)
+        out.append(torch.cat([p[:c] for p, c in zip(parts, counts)], 0))
+    return out[0], out[1]
+
+
+def train_surrogate(feats, tgts, *, epochs=30, batch=4, lr=5e-4, clip=1.0, val_frac=0.05, seed=0, log=print,
+                    device="cuda", conv=None, micro=1):
     """Trains the surrogate on resident data (features expanded to 16 channels per mini-batch): AdamW, one-cycle
     schedule, MSE on per-channel normalised targets, gradient-norm clipping. The last ``val_frac`` of the designs
-    are held back to report a validation loss per epoch."""
-    model = S.Surrogate("cuda", seed=seed)
+    are held back to report a validation loss per epoch.
+
+    Data parallel when torch.distributed is initialised: every rank holds the same design list, takes the
+    rank-th slice of each global mini-batch of ``batch`` designs (``batch`` divisible by the world size), and the
+    gradients are averaged by ONE all-reduce per step over a flat buffer (NCCL on GPUs). Normalisation
+    statistics and the shuffling are the same on every rank, so all ranks keep identical weights.
+
+    ``micro`` > 1 splits each rank's share into that many micro-batches with gradient accumulation (less memory
+    per step). The step's gradient is the sum over all world x micro slices divided by their count, so one process
+    with micro = k reproduces k ranks with micro = 1 bit for bit."""
+    rank, world = _world()
+    if batch % (world * micro):
+        raise ValueError(f"batch {batch} is not divisible by world size x micro-batches ({world} x {micro})")
+    model = S.Surrogate(device, seed=seed)
     n_all = feats.shape[0]
     n_val = int(round(val_frac * n_all)) if n_all > 20 else 0
     n = n_all - n_val
     mean = tgts[:n].mean(dim=(0, 1, 2, 3))
     std = tgts[:n].std(dim=(0, 1, 2, 3)).clamp_min(1e-6)
     model.norm = (mean, std)
-    opt = torch.optim.AdamW(model.parameters(), lr=lr, weight_decay=1e-4)
+    params = model.parameters()
+    opt = torch.optim.AdamW(params, lr=lr, weight_decay=1e-4)
     steps = epochs * math.ceil(n / batch)
     sched = torch.optim.lr_scheduler.OneCycleLR(opt, max_lr=lr, total_steps=steps, pct_start=0.1)
     g = torch.Generator().manual_seed(seed)
+    per = batch // world
+    sl = batch // (world * micro)  # designs per slice
+    flat = torch.zeros(sum(p.numel() for p in params), device=device)
 
     def inputs(idx):
-        x = torch.zeros((len(idx),) + tuple(feats.shape[1:4]) + (16,), dtype=S.BF16, device="cuda")
+        x = torch.zeros((len(idx),) + tuple(feats.shape[1:4]) + (16,), dtype=S.BF16, device=device)
         x[..., :S.IN_FEATURES] = feats[idx]
         return x
 
     hist = []
     for ep in range(epochs):
         order = torch.randperm(n, generator=g)
-        tot = torch.zeros((), device="cuda")
+        tot = torch.zeros((), device=device)
         for i in range(0, n, batch):
-            idx = order[i:i + batch].cuda()
-            y = (tgts[idx] - mean) / std
-            loss = torch.nn.functional.mse_loss(model.forward(inputs(idx))[..., :S.OUT_FIELDS], y)
+            gidx = order[i:i + batch]
             opt.zero_grad(set_to_none=True)
-            loss.backward()
-            torch.nn.utils.clip_grad_norm_(model.parameters(), clip)
+            for m in range(micro):
+                idx = gidx[(rank * micro + m) * sl:(rank * micro + m + 1) * sl].to(device)
+                if not len(idx):
+                    continue
+                y = (tgts[idx] - mean) / std
+                loss = torch.nn.functional.mse_loss(model.forward(inputs(idx), conv)[..., :S.OUT_FIELDS], y)
+                # slice weight: the step's gradient is the mean over its designs (a short last batch included)
+                k = len(idx) * world * micro / len(gidx)
+                (loss * k if k != 1.0 else loss).backward()
+                tot += loss.detach() * len(idx)
+            if world > 1:
+                # one all-reduce of every gradient per step
+                off = 0
+                for p in params:
+                    k = p.numel()
+                    flat[off:off + k] = p.grad.reshape(-1) if p.grad is not None else 0.0
+                    off += k
+                _allreduce_(flat)
+                off = 0
+                for p in params:
+                    k = p.numel()
+                    p.grad = flat[off:off + k].view_as(p).clone()
+                    off += k
+            if world * micro > 1:
+                for p in params:
+                    if p.grad is not None:
+                        p.grad /= world * micro
+            torch.nn.utils.clip_grad_norm_(params, clip)
             opt.step()
             sched.step()
-            tot += loss.detach() * len(idx)
+        _allreduce_(tot)
         rec = {"epoch": ep, "mse": float(tot) / n}
-        if n_val:
+        if n_val and rank == 0:
             with torch.no_grad():
-                vt = torch.zeros((), device="cuda")
+                vt = torch.zeros((), device=device)
                 for i in range(n, n_all, batch):
-                    idx = torch.arange(i, min(i + batch, n_all), device="cuda")
+                    idx = torch.arange(i, min(i + batch, n_all), device=device)
                     y = (tgts[idx] - mean) / std
-                    vt += torch.nn.functional.mse_loss(model.forward(inputs(idx))[..., :S.OUT_FIELDS], y,
+                    vt += torch.nn.functional.mse_loss(model.forward(inputs(idx), conv)[..., :S.OUT_FIELDS], y,
                                                        reduction="none").mean(dim=(1, 2, 3, 4)).sum()
                 rec["val_mse"] = float(vt) / n_val
         hist.append(rec)
-        if log:
+        if log and rank == 0:
             log(json.dumps(rec))
     return model, hist
 
@@ -256,17 +333,30 @@ def main(argv=None):
     ap.add_argument("--save", default=None, help="write the trained weights here (torch.save)")
     ap.add_argument("--load", default=None, help="skip data generation and training; load these weights")
     ap.add_argument("--out", default="warmstart.json")
+    ap.add_argument("--ddp", action="store_true",
+                    help="under torchrun: shard data generation over the ranks, gather it, train data-parallel (NCCL)")
     a = ap.parse_args(argv)
     report = {"args": vars(a)}
+    rank, world = 0, 1
+    if a.ddp:
+        import datetime
+        import os
+        import torch.distributed as dist
+        local = int(os.environ.get("LOCAL_RANK", 0))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(minutes=30))
+        rank, world = _world()
     if a.load:
         model = S.Surrogate("cuda")
         model.load_state_dict(torch.load(a.load))
     else:
         t = time.perf_counter()
-        feats, tgts, info = generate(list(range(a.train)), max_steps=a.gen_max_steps, tol=a.tol)
+        feats, tgts, info = generate(list(range(a.train))[rank::world], max_steps=a.gen_max_steps, tol=a.tol,
+                                     log=print if rank == 0 else None)
+        feats, tgts = gather_designs(feats, tgts)
         report["gen_s"] = time.perf_counter() - t
         report["gen"] = info
-        report["gen_converged"] = sum(i["converged"] for i in info)
+        report["gen_converged"] = sum(i["converged"] for i in info)  # this rank's shard
         report["gen_kept"] = int(feats.shape[0])
         print(json.dumps({k: report[k] for k in ("gen_s", "gen_converged", "gen_kept")}), flush=True)
         t = time.perf_counter()
@@ -275,8 +365,13 @@ def main(argv=None):
         report["train_s"] = time.perf_counter() - t
         report["train_mse"] = hist
         del feats, tgts
-        if a.save:
+        if a.save and rank == 0:
             torch.save(model.state_dict(), a.save)
+    if rank != 0:  # the comparison runs on rank 0
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+        return
     held = [HELDOUT_SEED0 + i for i in range(a.heldout)]
     report["eval"] = {}
     for tol in [float(t) for t in a.eval_tols.split(",")]:
@@ -294,6 +389,10 @@ def main(argv=None):
                           "dP_rel_max": bat["dP_rel_max"], "Rth_rel_max": bat["Rth_rel_max"],
                           "Rth_rel_median": bat["Rth_rel_median"],
                           "rescued": bat.get("warm_cold_tripped", {}).get("converged")}), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 if __name__ == "__main__":
