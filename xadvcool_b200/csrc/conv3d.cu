@@ -4,14 +4,14 @@
 // ci fastest), tap = (dz+1)*9 + (dy+1)*3 + (dx+1) for a 3x3x3 kernel (tap 0 only for 1x1x1); zero padding.
 //
 //   forward   out[v][co] = act( bias[co] + sum_{tap,ci} w[tap][co][ci] * in[v + off(tap)][ci] )
-//             GEMM M = voxels, N = Co, K = taps * Ci; each warp owns 16 voxels x all Co.
+//             GEMM M = voxels, N = Co, K = taps * Ci, on tcgen05 (128 voxels x Co per CTA, accumulator in TMEM).
 //   data grad the forward kernel applied to d_out with the flipped, transposed weights
 //             w'[26 - tap][ci][co] = w[tap][co][ci] (the adjoint of a zero-padded convolution).
 //   weight grad dw[tap][co][ci] = sum_v d_out[v][co] * in[v + off(tap)][ci]
 //             GEMM M = Co, N = Ci, K = voxels, split over voxel chunks; partials reduced in a fixed order.
 //
-// Tensor-core instruction: mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32. Ci and Co must be multiples of
-// 16 (the model pads its 4 input channels and 5 output channels to 16).
+// The weight gradient uses mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 tiles. Ci and Co must be multiples
+// of 16 (the model pads its 3 input channels and 5 output channels to 16).
 #include <cuda_bf16.h>
 
 #include <cstdint>
@@ -35,9 +35,6 @@ __device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-__device__ __forceinline__ uint32_t ld_pair(const __nv_bfloat16* p) {
-  return __ldg(reinterpret_cast<const unsigned int*>(p));
-}
 
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
 
@@ -64,75 +61,10 @@ __device__ __forceinline__ long long neighbour(const VoxelCoord& c, int dz, int 
   return (((long long)c.n * s.D + z) * s.H + y) * s.W + x;
 }
 
-// ---- forward / data grad -----------------------------------------------------------------------------
-// 4 warps per block, 16 voxels per warp, NT n-tiles of 8 output channels per warp: block (x, y) computes channels
-// [y*NT*8, (y+1)*NT*8) of voxels [64x, 64x + 64).
-template <int NT>
-__global__ void __launch_bounds__(128) conv_fwd_kernel(const __nv_bfloat16* __restrict__ in,
-                                                       const __nv_bfloat16* __restrict__ w,
-                                                       const float* __restrict__ bias, ConvShape s, int act,
-                                                       __nv_bfloat16* __restrict__ out_bf16,
-                                                       float* __restrict__ out_f32) {
-  const long long V = (long long)s.N * s.D * s.H * s.W;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long long v0 = ((long long)blockIdx.x * 4 + warp) * 16;
-  if (v0 >= V) return;
-  const int cobase = blockIdx.y * NT * 8;
-  const int r = lane >> 2, cq = (lane & 3) * 2;
-  // the two voxels (rows r and r+8) this lane loads A fragments for
-  const long long va = v0 + r, vb = v0 + r + 8;
-  const VoxelCoord ca = decode(va < V ? va : 0, s), cb = decode(vb < V ? vb : 0, s);
-  float acc[NT][4];
-#pragma unroll
-  for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
-  const int taps = s.ksize == 3 ? 27 : 1;
-  for (int tap = 0; tap < taps; ++tap) {
-    const int dz = s.ksize == 3 ? tap / 9 - 1 : 0, dy = s.ksize == 3 ? (tap / 3) % 3 - 1 : 0,
-              dx = s.ksize == 3 ? tap % 3 - 1 : 0;
-    const long long na = va < V ? neighbour(ca, dz, dy, dx, s) : -1;
-    const long long nb = vb < V ? neighbour(cb, dz, dy, dx, s) : -1;
-    const __nv_bfloat16* wt = w + (long long)tap * s.Co * s.Ci;
-    for (int ci0 = 0; ci0 < s.Ci; ci0 += 16) {
-      uint32_t a[4];
-      a[0] = na >= 0 ? ld_pair(in + na * s.Ci + ci0 + cq) : 0u;
-      a[1] = nb >= 0 ? ld_pair(in + nb * s.Ci + ci0 + cq) : 0u;
-      a[2] = na >= 0 ? ld_pair(in + na * s.Ci + ci0 + cq + 8) : 0u;
-      a[3] = nb >= 0 ? ld_pair(in + nb * s.Ci + ci0 + cq + 8) : 0u;
-#pragma unroll
-      for (int j = 0; j < NT; ++j) {
-        const __nv_bfloat16* wb = wt + (long long)(cobase + j * 8 + r) * s.Ci + ci0 + cq;
-        const uint32_t b[2] = {ld_pair(wb), ld_pair(wb + 8)};
-        mma_bf16_16816(acc[j], a, b);
-      }
-    }
-  }
-  // epilogue: rows r, r+8; columns j*8 + cq, +1
-#pragma unroll
-  for (int j = 0; j < NT; ++j) {
-    const int co = cobase + j * 8 + cq;
-    const float b0 = bias ? bias[co] : 0.0f, b1 = bias ? bias[co + 1] : 0.0f;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const long long v = h == 0 ? va : vb;
-      if (v >= V) continue;
-      float x0 = acc[j][2 * h] + b0, x1 = acc[j][2 * h + 1] + b1;
-      if (act == 1) {
-        x0 = gelu(x0);
-        x1 = gelu(x1);
-      }
-      if (out_bf16) {
-        __nv_bfloat162 pr = __floats2bfloat162_rn(x0, x1);
-        *reinterpret_cast<__nv_bfloat162*>(out_bf16 + v * s.Co + co) = pr;
-      } else {
-        *reinterpret_cast<float2*>(out_f32 + v * s.Co + co) = make_float2(x0, x1);
-      }
-    }
-  }
-}
-
 // ---- forward / data grad on the 5th-generation tensor cores (tcgen05) ------------------------------------
 // One CTA of 128 threads computes a 128-voxel x Co tile: D[128][Co] (FP32, in tensor memory) =
-// sum over K = taps x Ci of A[voxel][k] * B[co][k]. K is walked in stages of one tap x BK channels:
+// sum over K = taps x Ci of A[voxel][k] * B[co][k], k = tap * Ci + ci. K is walked in stages of 64 (eight 8-channel
+// chunks; a stage spans several taps when Ci < 64, and chunks past the end of K are zero):
 //   * all 128 threads gather the stage's operands into shared memory with 16-byte cp.async copies (zero-filled
 //     where the neighbour is outside the volume), A row r = voxel m0 + r, B row n = output channel n;
 //   * one thread issues the stage's BK/16 tcgen05.mma (kind::f16, BF16 in, FP32 accumulate) and a
@@ -213,9 +145,9 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+constexpr int kTcBK = 64;  // K per stage
 struct TcConv {
-  int BK;          // channels per stage (16..64, divides Ci)
-  int kt;          // stages of K: taps * Ci / BK
+  int kt;          // stages of K: ceil(taps * Ci / 64)
   uint32_t ncols;  // tensor-memory columns allocated (power of two >= max(32, Co))
 };
 
@@ -229,7 +161,8 @@ __global__ void __launch_bounds__(128, 1) conv_fwd_tc_kernel(const __nv_bfloat16
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int Co = s.Co, BK = t.BK, chunks = BK >> 3;
+  const int Co = s.Co, BK = kTcBK, chunks = kTcBK >> 3;
+  const int taps = s.ksize == 3 ? 27 : 1, Ktot = taps * s.Ci;
   const long long V = (long long)s.N * s.D * s.H * s.W;
   const long long m0 = (long long)blockIdx.x * kTcM;
   const uint32_t a_bytes = kTcM * BK * 2, b_bytes = (uint32_t)Co * BK * 2, stage_bytes = a_bytes + b_bytes;
@@ -262,22 +195,35 @@ __global__ void __launch_bounds__(128, 1) conv_fwd_tc_kernel(const __nv_bfloat16
   const long long v = m0 + tid;
   const bool vrow = v < V;
   const VoxelCoord vc = decode(vrow ? v : 0, s);
-  const int ci_chunks = s.Ci / BK;
   const uint32_t idesc = tc_idesc(Co);
 
   auto load_stage = [&](int k, int st) {
-    const int tap = k / ci_chunks, kc = k - tap * ci_chunks;
-    const int dz = s.ksize == 3 ? tap / 9 - 1 : 0, dy = s.ksize == 3 ? (tap / 3) % 3 - 1 : 0,
-              dx = s.ksize == 3 ? tap % 3 - 1 : 0;
-    const long long nb = vrow ? neighbour(vc, dz, dy, dx, s) : -1;
     const uint32_t a_st = sbase + (uint32_t)st * stage_bytes, b_st = a_st + a_bytes;
-    const __nv_bfloat16* asrc = nb >= 0 ? in + nb * s.Ci + kc * BK : in;
-    for (int j = 0; j < chunks; ++j)
-      cp_async16(a_st + (uint32_t)(j * kTcM + tid) * 16u, asrc + (nb >= 0 ? j * 8 : 0), nb >= 0 ? 16u : 0u);
-    const __nv_bfloat16* wt = w + ((long long)tap * Co) * s.Ci + kc * BK;
+    int cur_tap = -1;
+    long long nb = -1;
+    for (int j = 0; j < chunks; ++j) {
+      const int kk = k * kTcBK + j * 8;
+      const int tap = kk / s.Ci, ci = kk - tap * s.Ci;
+      if (tap != cur_tap) {  // neighbour of this thread's voxel for the chunk's tap
+        cur_tap = tap;
+        nb = -1;
+        if (vrow && tap < taps) {
+          const int dz = s.ksize == 3 ? tap / 9 - 1 : 0, dy = s.ksize == 3 ? (tap / 3) % 3 - 1 : 0,
+                    dx = s.ksize == 3 ? tap % 3 - 1 : 0;
+          nb = neighbour(vc, dz, dy, dx, s);
+        }
+      }
+      const bool ok = nb >= 0 && kk < Ktot;
+      cp_async16(a_st + (uint32_t)(j * kTcM + tid) * 16u, ok ? (const void*)(in + nb * s.Ci + ci) : (const void*)in,
+                 ok ? 16u : 0u);
+    }
     for (int e = tid; e < Co * chunks; e += 128) {
       const int n = e / chunks, j = e - n * chunks;
-      cp_async16(b_st + (uint32_t)(j * Co + n) * 16u, wt + (long long)n * s.Ci + j * 8, 16u);
+      const int kk = k * kTcBK + j * 8;
+      const int tap = kk / s.Ci, ci = kk - tap * s.Ci;
+      const bool ok = kk < Ktot;
+      const __nv_bfloat16* src = ok ? w + ((long long)tap * Co + n) * s.Ci + ci : w;
+      cp_async16(b_st + (uint32_t)(j * Co + n) * 16u, src, ok ? 16u : 0u);
     }
   };
   auto mma_stage = [&](int k, int st) {
@@ -487,16 +433,14 @@ int xac_conv3d_forward(const void* in, int N, int D, int H, int W, int Ci, const
   XAC_REQUIRE(activation == 0 || activation == 1, "xac_conv3d_forward: activation must be 0 (none) or 1 (GELU)");
   const long long V = (long long)N * D * H * W;
   TcConv t;
-  t.BK = 64;
-  while (Ci % t.BK != 0) t.BK -= 16;  // 64, 48, 32 or 16
-  t.kt = (ksize == 3 ? 27 : 1) * (Ci / t.BK);
+  t.kt = ((ksize == 3 ? 27 : 1) * Ci + kTcBK - 1) / kTcBK;
   t.ncols = 32;
   while ((int)t.ncols < Co) t.ncols <<= 1;
-  const size_t smem = (size_t)kTcStages * (kTcM + Co) * t.BK * 2;
+  const size_t smem = (size_t)kTcStages * (kTcM + Co) * kTcBK * 2;
   static bool attr_set = false;  // the attribute is per device function; set once per process
   if (!attr_set) {
     XAC_CUDA(cudaFuncSetAttribute(conv_fwd_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)((size_t)kTcStages * (kTcM + 256) * 64 * 2)));
+                                  (int)((size_t)kTcStages * (kTcM + 256) * kTcBK * 2)));
     attr_set = true;
   }
   const unsigned grid = (unsigned)((V + kTcM - 1) / kTcM);
