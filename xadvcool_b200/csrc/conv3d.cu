@@ -63,8 +63,7 @@ __device__ __forceinline__ long long neighbour(const VoxelCoord& c, int dz, int 
 
 // ---- forward / data grad on the 5th-generation tensor cores (tcgen05) ------------------------------------
 // One CTA of 128 threads computes a 128-voxel x Co tile: D[128][Co] (FP32, in tensor memory) =
-// sum over K = taps x Ci of A[voxel][k] * B[co][k], k = tap * Ci + ci. K is walked in stages of 64 (eight 8-channel
-// chunks; a stage spans several taps when Ci < 64, and chunks past the end of K are zero):
+// sum over K = taps x Ci of A[voxel][k] * B[co][k]. K is walked in stages of one tap x BK channels:
 //   * all 128 threads gather the stage's operands into shared memory with 16-byte cp.async copies (zero-filled
 //     where the neighbour is outside the volume), A row r = voxel m0 + r, B row n = output channel n;
 //   * one thread issues the stage's BK/16 tcgen05.mma (kind::f16, BF16 in, FP32 accumulate) and a
@@ -145,9 +144,9 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-constexpr int kTcBK = 64;  // K per stage
 struct TcConv {
-  int kt;          // stages of K: ceil(taps * Ci / 64)
+  int BK;          // channels per stage (16..64, divides Ci)
+  int kt;          // stages of K: taps * Ci / BK
   uint32_t ncols;  // tensor-memory columns allocated (power of two >= max(32, Co))
 };
 
@@ -161,8 +160,7 @@ __global__ void __launch_bounds__(128, 1) conv_fwd_tc_kernel(const __nv_bfloat16
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int Co = s.Co, BK = kTcBK, chunks = kTcBK >> 3;
-  const int taps = s.ksize == 3 ? 27 : 1, Ktot = taps * s.Ci;
+  const int Co = s.Co, BK = t.BK, chunks = BK >> 3;
   const long long V = (long long)s.N * s.D * s.H * s.W;
   const long long m0 = (long long)blockIdx.x * kTcM;
   const uint32_t a_bytes = kTcM * BK * 2, b_bytes = (uint32_t)Co * BK * 2, stage_bytes = a_bytes + b_bytes;
@@ -195,35 +193,22 @@ __global__ void __launch_bounds__(128, 1) conv_fwd_tc_kernel(const __nv_bfloat16
   const long long v = m0 + tid;
   const bool vrow = v < V;
   const VoxelCoord vc = decode(vrow ? v : 0, s);
+  const int ci_chunks = s.Ci / BK;
   const uint32_t idesc = tc_idesc(Co);
 
   auto load_stage = [&](int k, int st) {
+    const int tap = k / ci_chunks, kc = k - tap * ci_chunks;
+    const int dz = s.ksize == 3 ? tap / 9 - 1 : 0, dy = s.ksize == 3 ? (tap / 3) % 3 - 1 : 0,
+              dx = s.ksize == 3 ? tap % 3 - 1 : 0;
+    const long long nb = vrow ? neighbour(vc, dz, dy, dx, s) : -1;
     const uint32_t a_st = sbase + (uint32_t)st * stage_bytes, b_st = a_st + a_bytes;
-    int cur_tap = -1;
-    long long nb = -1;
-    for (int j = 0; j < chunks; ++j) {
-      const int kk = k * kTcBK + j * 8;
-      const int tap = kk / s.Ci, ci = kk - tap * s.Ci;
-      if (tap != cur_tap) {  // neighbour of this thread's voxel for the chunk's tap
-        cur_tap = tap;
-        nb = -1;
-        if (vrow && tap < taps) {
-          const int dz = s.ksize == 3 ? tap / 9 - 1 : 0, dy = s.ksize == 3 ? (tap / 3) % 3 - 1 : 0,
-                    dx = s.ksize == 3 ? tap % 3 - 1 : 0;
-          nb = neighbour(vc, dz, dy, dx, s);
-        }
-      }
-      const bool ok = nb >= 0 && kk < Ktot;
-      cp_async16(a_st + (uint32_t)(j * kTcM + tid) * 16u, ok ? (const void*)(in + nb * s.Ci + ci) : (const void*)in,
-                 ok ? 16u : 0u);
-    }
+    const __nv_bfloat16* asrc = nb >= 0 ? in + nb * s.Ci + kc * BK : in;
+    for (int j = 0; j < chunks; ++j)
+      cp_async16(a_st + (uint32_t)(j * kTcM + tid) * 16u, asrc + (nb >= 0 ? j * 8 : 0), nb >= 0 ? 16u : 0u);
+    const __nv_bfloat16* wt = w + ((long long)tap * Co) * s.Ci + kc * BK;
     for (int e = tid; e < Co * chunks; e += 128) {
       const int n = e / chunks, j = e - n * chunks;
-      const int kk = k * kTcBK + j * 8;
-      const int tap = kk / s.Ci, ci = kk - tap * s.Ci;
-      const bool ok = kk < Ktot;
-      const __nv_bfloat16* src = ok ? w + ((long long)tap * Co + n) * s.Ci + ci : w;
-      cp_async16(b_st + (uint32_t)(j * Co + n) * 16u, src, ok ? 16u : 0u);
+      cp_async16(b_st + (uint32_t)(j * Co + n) * 16u, wt + (long long)n * s.Ci + j * 8, 16u);
     }
   };
   auto mma_stage = [&](int k, int st) {
@@ -433,14 +418,16 @@ int xac_conv3d_forward(const void* in, int N, int D, int H, int W, int Ci, const
   XAC_REQUIRE(activation == 0 || activation == 1, "xac_conv3d_forward: activation must be 0 (none) or 1 (GELU)");
   const long long V = (long long)N * D * H * W;
   TcConv t;
-  t.kt = ((ksize == 3 ? 27 : 1) * Ci + kTcBK - 1) / kTcBK;
+  t.BK = 64;
+  while (Ci % t.BK != 0) t.BK -= 16;  // 64, 48, 32 or 16
+  t.kt = (ksize == 3 ? 27 : 1) * (Ci / t.BK);
   t.ncols = 32;
   while ((int)t.ncols < Co) t.ncols <<= 1;
-  const size_t smem = (size_t)kTcStages * (kTcM + Co) * kTcBK * 2;
+  const size_t smem = (size_t)kTcStages * (kTcM + Co) * t.BK * 2;
   static bool attr_set = false;  // the attribute is per device function; set once per process
   if (!attr_set) {
     XAC_CUDA(cudaFuncSetAttribute(conv_fwd_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)((size_t)kTcStages * (kTcM + 256) * kTcBK * 2)));
+                                  (int)((size_t)kTcStages * (kTcM + 256) * 64 * 2)));
     attr_set = true;
   }
   const unsigned grid = (unsigned)((V + kTcM - 1) / kTcM);
