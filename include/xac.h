@@ -226,6 +226,29 @@ int xac_lattice_scalars(xac_lattice *lat, const xac_scalar_params *params, doubl
 int xac_scalars_fields(const float *rho, const float *u, const float *T, const int32_t *mask, int nx, int ny, int nz,
                        const xac_scalar_params *params, double out_host[XAC_NSCALARS], void *stream);
 /* Raw population state for checkpoint / restart. */
+/* Physical validators of the current fields (analyze_dataset.py:184-323) as FP64 device reductions; out_host
+ * receives XAC_NVALIDATE raw values in the order of the XAC_VAL_* slots below, from which
+ * xadvcool_b200.validate forms the reference's checks (mass and energy balance, Mach, density deviation,
+ * temperature lower bound, pressure-drop sign, divergence). */
+#define XAC_VAL_MDOT_IN 0     /* sum rho*ux, non-solid cells of plane x = 1 */
+#define XAC_VAL_MDOT_OUT 1    /* the same, plane x = nx-2 */
+#define XAC_VAL_MAXV 2        /* max |u| over non-solid cells */
+#define XAC_VAL_RHODEV 3      /* max |rho - 1| over non-solid cells */
+#define XAC_VAL_TMIN 4        /* min T over non-solid cells */
+#define XAC_VAL_NFLUID 5
+#define XAC_VAL_RHO1_ALL 6    /* sum rho over all cells of plane x = 1 */
+#define XAC_VAL_RHO2_ALL 7    /* the same, plane x = nx-2 */
+#define XAC_VAL_DIV_SUM 8     /* sum |div u| over non-solid interior cells (central differences) */
+#define XAC_VAL_DIV_MAX 9
+#define XAC_VAL_DIV_N 10
+#define XAC_VAL_QSRC 11       /* sum of the injected heat source (heat_power x normalised map) */
+#define XAC_VAL_ADV_IN 12     /* sum ux over inlet cells of plane x = 0 */
+#define XAC_VAL_ADV_OUT 13    /* sum ux*T over outlet cells of plane x = nx-1 */
+#define XAC_VAL_DIFF_IN 14    /* sum over plane x = 1 of -k (T[1] - T[0]), k = (tau_th - 0.5)/3 of the cell */
+#define XAC_VAL_DIFF_OUT 15   /* sum over plane x = nx-2 of -k (T[nx-1] - T[nx-2]) */
+#define XAC_NVALIDATE 16
+int xac_lattice_validate(xac_lattice *lat, double *out_host, void *stream);
+
 int xac_lattice_state_bytes(const xac_lattice *lat, size_t *bytes);
 int xac_lattice_save_state(xac_lattice *lat, void *host_dst, size_t bytes, void *stream);
 int xac_lattice_load_state(xac_lattice *lat, const void *host_src, size_t bytes, void *stream);

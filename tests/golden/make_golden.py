@@ -5,6 +5,8 @@ does not, so the outputs are committed).
                   states, and of the ten heat maps (src/geometry.py, imported with a pyvista stub).
 * metrics.json  — compute_macroscopic_metrics() (generate_dataset.py:80-179, imported with h5py and
                   src.simulation stubs) on seeded synthetic fields (fields rebuilt by ``synthetic_fields``).
+* validate.json — validate_sample() (analyze_dataset.py:184-323, imported with h5py and matplotlib stubs; the
+                  HDF5 group is served from memory) on the seeded cases of oracle.validate_ref.validation_case.
 * parquet_rows.json — stratified rows of dataset/metadata.parquet (inputs and golden scalars of the
                   reference's GPU runs), excluding gaussian_hotspots rows whose seed is process-salted.
 
@@ -42,6 +44,21 @@ def synthetic_fields(seed: int, shape=(148, 128, 32)):
     return rho, u, T
 
 
+def validation_case(seed: int):
+    """A seeded small gyroid design with smooth fields consistent with solver output (solid rho = 1, u = 0),
+    its heat map normalised to 1, and fixed dataset attributes."""
+    from xadvcool_b200.designs import gyroid_design
+    mask, hs, u_in, _ = gyroid_design(seed, nx=48, ny=24, nz=16, buf=6)
+    rho, u, T = synthetic_fields(100 + seed, shape=mask.shape)
+    solid = mask == 1
+    rho[solid] = 1.0
+    u[solid] = 0.0
+    hs = (hs / hs.max()).astype(np.float32)
+    attrs = {"heat_power": 0.1, "Pr": 7.0, "k_ratio": 628.0, "tau_fluid": 0.55, "Nu": 12.5 + seed,
+             "f_friction": 0.8, "Re": 30.0 + seed}
+    return mask, rho, u, T, hs, attrs
+
+
 def _sha(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
@@ -56,6 +73,62 @@ def _import_reference(ref: Path):
     import src.geometry as geometry  # noqa: E402
     import generate_dataset as gd  # noqa: E402
     return geometry, gd
+
+
+def _validate_reference(ref: Path):
+    """analyze_dataset.validate_sample with its HDF5 reader and plotting imports stubbed: the returned function
+    runs the reference code on in-memory arrays."""
+    sys.path.insert(0, str(ref))
+    store = {}
+
+    class _Ds:
+        def __init__(self, a):
+            self.a = a
+
+        def __getitem__(self, k):
+            return self.a
+
+    class _Grp:
+        def __init__(self, d, attrs):
+            self.d, self.attrs = d, attrs
+
+        def __getitem__(self, k):
+            return _Ds(self.d[k])
+
+    class _File:
+        def __init__(self, path, mode="r"):
+            self.path = path
+
+        def __enter__(self):
+            return self
+
+        def __exit__(self, *a):
+            return False
+
+        def __getitem__(self, sid):
+            d, attrs = store[sid]
+            return _Grp(d, attrs)
+
+    h5 = types.ModuleType("h5py")
+    h5.File = _File
+    sys.modules["h5py"] = h5
+    mpl = types.ModuleType("matplotlib")
+    mpl.use = lambda *a, **k: None
+    mpl.rcParams = {}
+    sys.modules["matplotlib"] = mpl
+    for sub in ("pyplot", "ticker", "colors", "gridspec", "cm", "patches", "lines", "collections"):
+        m = types.ModuleType("matplotlib." + sub)
+        m.__getattr__ = lambda name: object  # any plotting name imports as a placeholder
+        setattr(mpl, sub, m)
+        sys.modules["matplotlib." + sub] = m
+    import analyze_dataset as ad  # noqa: E402
+
+    def run(mask, rho, u, T, hs, attrs):
+        store["s"] = ({"mask": mask, "velocity": u, "temperature": T, "pressure": rho / 3.0, "heat_source": hs},
+                      dict(attrs))
+        return ad.validate_sample("unused.h5", "s")
+
+    return run
 
 
 def main(ref: Path):
@@ -124,6 +197,16 @@ def main(ref: Path):
                        "pressure_drop_all": float(np.mean(rho[1]) - np.mean(rho[-2])) / 3.0,
                        "metrics": {k2: float(v) for k2, v in res.items()}})
     (HERE / "metrics.json").write_text(json.dumps(mcases, indent=1))
+
+    # ---- validators: the reference's validate_sample on seeded small designs (oracle.validate_ref.validation_case)
+    run = _validate_reference(ref)
+    vcases = []
+    for seed in range(3):
+        mask, rho, u, T, hs, attrs = validation_case(seed)
+        res = run(mask, rho, u, T, hs, attrs)
+        vcases.append({"seed": seed, "checks": {k: (bool(v) if isinstance(v, (bool, np.bool_)) else float(v))
+                                                for k, v in res.items() if k != "sample_id"}})
+    (HERE / "validate.json").write_text(json.dumps(vcases, indent=1))
     print(f"wrote {len(out_rows)} rows, {len(designs)} masks, {len(heat)} heat maps, {len(mcases)} metric cases")
 
 

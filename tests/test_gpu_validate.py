@@ -1,0 +1,47 @@
+"""The validators' FP64 device reductions (xac_lattice_validate) on a lattice holding the seeded fields, against
+the numpy restatement and the reference's checks (tests/golden/validate.json)."""
+import json
+from pathlib import Path
+
+import pytest
+import torch
+
+from oracle.validate_ref import raw_sums
+from tests.golden.make_golden import validation_case
+from xadvcool_b200.lattice import Lattice
+from xadvcool_b200.validate import checks_from_raw, validate
+
+pytestmark = pytest.mark.gpu
+GOLDEN = json.loads((Path(__file__).parent / "golden" / "validate.json").read_text())
+
+
+@pytest.mark.parametrize("case", GOLDEN, ids=lambda c: f"seed{c['seed']}")
+def test_device_reductions_match(case, cuda):
+    mask, rho, u, T, hs, attrs = validation_case(case["seed"])
+    lat = Lattice(mask, heat_source=hs, tau_fluid=attrs["tau_fluid"], heat_power=attrs["heat_power"],
+                  Pr=attrs["Pr"], k_ratio=attrs["k_ratio"])
+    lat.init_fields(torch.from_numpy(rho).cuda(), torch.from_numpy(u).cuda(), torch.from_numpy(T).cuda())
+    raw = lat.validate_raw()
+    ref = raw_sums(mask, rho, u, T, hs, attrs["heat_power"])
+    for k, v in ref.items():
+        assert abs(raw[k] - v) <= 1e-6 * max(abs(v), 1e-9), (k, raw[k], v)
+    got = validate(lat, attrs=attrs)
+    for k, v in case["checks"].items():
+        if isinstance(v, bool):
+            assert bool(got[k]) == v, k
+        else:
+            # absolute tolerances for the differences of float32 sums in the reference (see test_validate.py)
+            extra = {"delta_P": 1e-6, "mass_err": 1e-6, "energy_err": 1e-5}.get(k, 0.0)
+            assert abs(got[k] - v) <= 2e-6 * max(abs(v), 1e-12) + extra, (k, got[k], v)
+    lat.close()
+
+
+def test_validate_after_a_solve(cuda):
+    """On real solver output the checks are defined and the flow ones pass for a short, stable run."""
+    from xadvcool_b200.designs import straight_fin_plate
+    lat = Lattice(straight_fin_plate(), tau_fluid=0.6, u_inlet_val=0.03, heat_power=1e-4)
+    lat.step(400)
+    c = validate(lat, buf=8, core_nx=48, core_ny=32)
+    assert c["mach_pass"] and c["T_lb_warn"]
+    assert all(k in c for k in ("mass_err", "energy_err", "mean_div", "delta_P", "f_Re"))
+    lat.close()

@@ -29,6 +29,11 @@ SCALAR_NAMES = [
 ]
 NSCALARS = len(SCALAR_NAMES)
 
+# validator slots (XAC_VAL_*)
+VALIDATE_NAMES = ["mdot_in", "mdot_out", "max_v", "rho_dev", "T_min", "n_fluid", "rho1_all", "rho2_all", "div_sum",
+                  "div_max", "div_n", "q_src", "adv_in", "adv_out", "diff_in", "diff_out"]
+NVALIDATE = len(VALIDATE_NAMES)
+
 
 class XacError(RuntimeError):
     def __init__(self, code: int, msg: str):
@@ -106,6 +111,7 @@ SIGNATURES = {
     "xac_lattice_save_state": [_vp, _vp, C.c_size_t, _vp],
     "xac_lattice_load_state": [_vp, _vp, C.c_size_t, _vp],
     "xac_lattice_run": [_vp, C.POINTER(RunOpts), C.POINTER(RunResult), _vp],
+    "xac_lattice_validate": [_vp, _vp, _vp],
     "xac_conv3d_forward": [_vp, _i, _i, _i, _i, _i, _vp, _vp, _i, _i, _i, _vp, _vp, _vp],
     "xac_conv3d_weight_grad": [_vp, _i, _i, _i, _i, _i, _vp, _i, _i, _vp, _vp, _vp, _vp],
     "xac_conv3d_partial_floats": [_i, _i, _i, _i, _i, _i, _i, C.POINTER(C.c_longlong)],

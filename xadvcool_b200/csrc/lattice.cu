@@ -713,6 +713,26 @@ int xac_lattice_scalars(xac_lattice* lat, const xac_scalar_params* prm, double* 
   return XAC_OK;
 }
 
+int xac_lattice_validate(xac_lattice* lat, double* out_host, void* stream) {
+  XAC_REQUIRE(lat && out_host, "xac_lattice_validate: null pointer");
+  LatticeImpl& L = lat->impl;
+  std::lock_guard<std::mutex> g(L.mu);
+  cudaStream_t s = as_stream(stream);
+  int r = L.finalize_T(s);  // rho and u are written by the last step of every step call
+  if (r != XAC_OK) return r;
+  // analyze_dataset.py:274-281 in double
+  const double tth_f = 0.5 + (L.tau_fluid - 0.5) / L.Pr, tth_s = 0.5 + L.k_ratio * (tth_f - 0.5);
+  const double k_fluid = (1.0 / 3.0) * (tth_f - 0.5), k_solid = (1.0 / 3.0) * (tth_s - 0.5);
+  const auto spec = validate_spec();
+  validate_partials_kernel<<<L.red_blocks, kBlock, 0, s>>>(L.view(), L.qsrc, k_fluid, k_solid, spec, L.rows);
+  combine_rows_kernel<kNValidate><<<1, 32 * kNValidate, 0, s>>>(L.rows, L.red_blocks, spec, L.red_out);
+  XAC_CUDA(cudaGetLastError());
+  XAC_CUDA(cudaMemcpyAsync(L.host_out, L.red_out, kNValidate * sizeof(double), cudaMemcpyDeviceToHost, s));
+  XAC_CUDA(cudaStreamSynchronize(s));
+  std::memcpy(out_host, L.host_out, kNValidate * sizeof(double));
+  return XAC_OK;
+}
+
 int xac_lattice_state_bytes(const xac_lattice* lat, size_t* bytes) {
   XAC_REQUIRE(lat && bytes, "xac_lattice_state_bytes: null pointer");
   const LatticeImpl& L = lat->impl;

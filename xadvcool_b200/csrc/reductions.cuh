@@ -286,4 +286,90 @@ static __global__ void __launch_bounds__(256) metric_partials_kernel(FieldView v
   block_reduce<kNMetrics>(acc, spec, rows + (long long)blockIdx.x * kNMetrics);
 }
 
+// ---- physical validators (analyze_dataset.py:184-323) ------------------------------------------
+enum ValidateSlot : int {
+  kV_MDOT_IN = 0,  // sum rho*ux over non-solid cells of plane x = 1            (:201-206)
+  kV_MDOT_OUT,     // the same over plane x = nx-2
+  kV_MAXV,         // max |u| over non-solid cells                             (:214-216)
+  kV_RHODEV,       // max |rho - 1| over non-solid cells                       (:222)
+  kV_TMIN,         // min T over non-solid cells                               (:229)
+  kV_NFLUID,       // non-solid cells
+  kV_RHO1_ALL,     // sum rho over all cells of plane x = 1                    (:236-238)
+  kV_RHO2_ALL,     // the same over plane x = nx-2
+  kV_DIV_SUM,      // sum |div u| over non-solid interior cells (central differences, :257-263)
+  kV_DIV_MAX,
+  kV_DIV_N,
+  kV_QSRC,         // sum of the injected source heat_power * map over all cells
+  kV_ADV_IN,       // sum ux over inlet cells of plane x = 0                   (:294-297)
+  kV_ADV_OUT,      // sum ux*T over outlet cells of plane x = nx-1
+  kV_DIFF_IN,      // sum over plane x = 1 of -k(cell) * (T[1] - T[0])          (:300-306)
+  kV_DIFF_OUT,     // sum over plane x = nx-2 of -k(cell) * (T[nx-1] - T[nx-2])
+  kNValidate
+};
+
+inline ReduceSpec<kNValidate> validate_spec() {
+  ReduceSpec<kNValidate> s{};
+  for (int k = 0; k < kNValidate; ++k) s.op[k] = kSum;
+  s.op[kV_MAXV] = kMax;
+  s.op[kV_RHODEV] = kMax;
+  s.op[kV_TMIN] = kMin;
+  s.op[kV_DIV_MAX] = kMax;
+  return s;
+}
+
+// q: heat source per cell (compact order of the view, may be null); k_fluid / k_solid: thermal conductivities
+// (tau_th - 0.5) / 3 of the two phases (:280-281). Per-cell differences are formed in float32 like the
+// reference's float32 arrays; sums are FP64.
+static __global__ void __launch_bounds__(256) validate_partials_kernel(FieldView v, const float* __restrict__ q,
+                                                                double k_fluid, double k_solid,
+                                                                ReduceSpec<kNValidate> spec,
+                                                                double* __restrict__ rows) {
+  double acc[kNValidate];
+#pragma unroll
+  for (int k = 0; k < kNValidate; ++k) acc[k] = identity(spec.op[k]);
+  const long long n = (long long)v.nx * v.ny * v.nz;
+  const int nx = v.nx, ny = v.ny, nz = v.nz;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx);
+    const long long t = i / nx;
+    const int y = (int)(t % ny), z = (int)(t / ny);
+    const long long cell = x * v.sx + y * v.sy + z * v.sz;
+    const int m = view_type(v, cell);
+    const bool fluid = m != kSolid;
+    const float ux = v.ux[cell * v.ustride], uy = v.uy[cell * v.ustride], uz = v.uz[cell * v.ustride];
+    const float r = v.rho[cell], T = v.T[cell];
+    if (q) acc[kV_QSRC] += (double)q[i];
+    if (x == 1) {
+      acc[kV_RHO1_ALL] += (double)r;
+      if (fluid) acc[kV_MDOT_IN] += (double)(r * ux);
+      acc[kV_DIFF_IN] += -(fluid ? k_fluid : k_solid) * (double)(T - v.T[cell - v.sx]);
+    }
+    if (x == nx - 2) {
+      acc[kV_RHO2_ALL] += (double)r;
+      if (fluid) acc[kV_MDOT_OUT] += (double)(r * ux);
+      acc[kV_DIFF_OUT] += -(fluid ? k_fluid : k_solid) * (double)(v.T[cell + v.sx] - T);
+    }
+    if (x == 0 && m == kInlet) acc[kV_ADV_IN] += (double)ux;
+    if (x == nx - 1 && m == kOutlet) acc[kV_ADV_OUT] += (double)(ux * T);
+    if (fluid) {
+      acc[kV_NFLUID] += 1.0;
+      const float vm = sqrtf(ux * ux + uy * uy + uz * uz);
+      acc[kV_MAXV] = fmax(acc[kV_MAXV], (double)vm);
+      acc[kV_RHODEV] = fmax(acc[kV_RHODEV], (double)fabsf(r - 1.0f));
+      acc[kV_TMIN] = fmin(acc[kV_TMIN], (double)T);
+      if (x >= 1 && x < nx - 1 && y >= 1 && y < ny - 1 && z >= 1 && z < nz - 1) {
+        const long long us = v.ustride;
+        const float dux = (v.ux[(cell + v.sx) * us] - v.ux[(cell - v.sx) * us]) / 2.0f;
+        const float duy = (v.uy[(cell + v.sy) * us] - v.uy[(cell - v.sy) * us]) / 2.0f;
+        const float duz = (v.uz[(cell + v.sz) * us] - v.uz[(cell - v.sz) * us]) / 2.0f;
+        const double d = fabs((double)((dux + duy) + duz));
+        acc[kV_DIV_SUM] += d;
+        acc[kV_DIV_MAX] = fmax(acc[kV_DIV_MAX], d);
+        acc[kV_DIV_N] += 1.0;
+      }
+    }
+  }
+  block_reduce<kNValidate>(acc, spec, rows + (long long)blockIdx.x * kNValidate);
+}
+
 }  // namespace xac

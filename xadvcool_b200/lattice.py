@@ -148,6 +148,13 @@ class Lattice:
             _capi.call("xac_lattice_scalars", self._h, C.byref(p), out.ctypes.data, stream_ptr(self.device))
         return dict(zip(_capi.SCALAR_NAMES, out.tolist()))
 
+    def validate_raw(self) -> dict:
+        """FP64 device reductions behind the physical validators (XAC_VAL_* slots by name)."""
+        out = np.zeros(_capi.NVALIDATE, dtype=np.float64)
+        with torch.cuda.device(self.device):
+            _capi.call("xac_lattice_validate", self._h, out.ctypes.data, stream_ptr(self.device))
+        return dict(zip(_capi.VALIDATE_NAMES, out.tolist()))
+
     # -- native loop -----------------------------------------------------------------------------
     def run(self, max_steps=40000, stats_every=100, tol_ke=1e-7, tol_T=1e-7, pump_mode="constant_flow",
             target_power=1.0, min_steps=0) -> dict:
