@@ -45,3 +45,26 @@ def test_validate_after_a_solve(cuda):
     assert c["mach_pass"] and c["T_lb_warn"]
     assert all(k in c for k in ("mass_err", "energy_err", "mean_div", "delta_P", "f_Re"))
     lat.close()
+
+
+def test_dataset_writer_from_a_lattice(cuda, tmp_path):
+    """A solved lattice written with the reference's schema: the row's scalars are the device scalars and the
+    sample's fields are the lattice's fields."""
+    import numpy as np
+    import pandas as pd
+    from xadvcool_b200 import dataset as D
+    from xadvcool_b200.designs import gyroid_design
+    mask, hs, u_in, info = gyroid_design(2, nx=48, ny=24, nz=16, buf=6)
+    design = dict(tau_fluid=0.56, u_inlet_val=u_in, heat_power=0.05, heat_source=hs, design_name="gyroid")
+    lat = Lattice(mask, heat_source=hs, tau_fluid=0.56, u_inlet_val=u_in, heat_power=0.05)
+    res = lat.run(max_steps=300, tol_ke=0.0, tol_T=0.0)
+    w = D.DatasetWriter(tmp_path)
+    row = w.add_lattice("g2", lat, design, res, elapsed_s=0.1, buf=6)
+    w.close()
+    sc = lat.scalars(buf=6, core_nx=36, core_ny=24)
+    assert row["Nu"] == sc["Nu"] and row["sim_steps"] == 300 and row["grid_cells"] == mask.size
+    data, attrs = D.load_sample(tmp_path / "samples" / "g2.npz")
+    rho, u, T = (t.cpu().numpy() for t in lat.fields())
+    assert np.array_equal(data["temperature"], T) and np.array_equal(data["velocity"], u)
+    assert pd.read_parquet(tmp_path / "metadata.parquet")["sample_id"].tolist() == ["g2"]
+    lat.close()
