@@ -311,8 +311,9 @@ int xac_batch_lattice(xac_batch *batch, int i, xac_lattice **lat);
 /* Threads per block (64, 128, 256; also the cells per tile) and steps per persistent launch. */
 int xac_batch_tune(xac_batch *batch, int block, int steps_per_launch);
 int xac_batch_get_tune(const xac_batch *batch, int *block, int *steps_per_launch);
-/* Run every design from step 0 to convergence, divergence or opts->max_steps (constant_power must be 0);
- * results[i] receives design i's outcome. */
+/* Run every design from step 0 to convergence, divergence or opts->max_steps; results[i] receives design i's
+ * outcome. With opts->constant_power the reference's pump controller (simulation.py:139-146) runs inside the
+ * persistent kernel on each design's stats, exactly as xac_lattice_run runs it for one lattice. */
 int xac_batch_run(xac_batch *batch, const xac_run_opts *opts, xac_run_result *results, void *stream);
 
 #ifdef __cplusplus

@@ -77,3 +77,25 @@ def test_batch_rejects_bad_input(cuda):
     b.run(max_steps=200, stats_every=100)
     with pytest.raises(Exception):  # designs must restart from step 0
         b.run(max_steps=200, stats_every=100)
+
+
+@pytest.mark.parametrize("spl", [1000, 300])
+def test_batch_constant_power_equals_solo(spl, cuda):
+    """The pump controller inside the persistent kernel (src/simulation.py:139-146) gives each design the inlet
+    history, step count and fields of its solo constant-power solve, bit for bit."""
+    ds = small_designs()[:3]
+    run = dict(max_steps=3000, stats_every=100, tol_ke=1e-6, tol_T=1e-6, pump_mode="constant_power",
+               target_power=0.02)
+    b = Batch(ds)
+    b.tune(128, spl)
+    res = b.run(**run)
+    for i, d in enumerate(ds):
+        r_solo, f_solo = solo(d, **run)
+        assert res[i]["steps"] == r_solo["steps"]
+        assert res[i]["u_inlet_final"] == r_solo["u_inlet_final"]
+        assert res[i]["u_inlet_final"] != pytest.approx(d["u_inlet_val"], rel=1e-3)  # the pump acted
+        lat = b.lattice(i)
+        assert lat.get_inlet() == pytest.approx(r_solo["u_inlet_final"], rel=0, abs=0)
+        for x, y in zip([t.cpu().numpy() for t in lat.fields()], f_solo):
+            assert np.array_equal(x, y)
+    b.close()

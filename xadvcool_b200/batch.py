@@ -84,12 +84,17 @@ class Batch:
         _capi.call("xac_batch_get_tune", self._h, C.byref(b), C.byref(s))
         return int(b.value), int(s.value)
 
-    def run(self, max_steps=30000, stats_every=100, tol_ke=1e-7, tol_T=1e-7, min_steps=0) -> list:
-        """``min_steps`` > 0 replaces the reference's minimum run length (warm-started designs)."""
-        o = _capi.RunOpts(int(max_steps), int(stats_every), float(tol_ke), float(tol_T), 0, 1.0, int(min_steps))
+    def run(self, max_steps=30000, stats_every=100, tol_ke=1e-7, tol_T=1e-7, min_steps=0, pump_mode="constant_flow",
+            target_power=1.0) -> list:
+        """``min_steps`` > 0 replaces the reference's minimum run length (warm-started designs); ``pump_mode``
+        "constant_power" runs the reference's pump controller (src/simulation.py:139-146) on every design."""
+        if pump_mode not in ("constant_flow", "constant_power"):
+            raise ValueError(f"unknown pump_mode {pump_mode!r}")
+        o = _capi.RunOpts(int(max_steps), int(stats_every), float(tol_ke), float(tol_T),
+                          1 if pump_mode == "constant_power" else 0, float(target_power), int(min_steps))
         res = (_capi.RunResult * self.n)()
         with torch.cuda.device(self.device):
             _capi.call("xac_batch_run", self._h, C.byref(o), res, stream_ptr(self.device))
         return [{"steps": int(r.steps), "converged": bool(r.converged), "diverged": bool(r.diverged),
-                 "d_ke": r.d_ke, "dT_conv": r.dT_conv, "dQ_conv": r.dQ_conv,
+                 "d_ke": r.d_ke, "dT_conv": r.dT_conv, "dQ_conv": r.dQ_conv, "u_inlet_final": r.u_inlet_final,
                  "last_stats": np.array(r.last_stats[:], dtype=np.float64)} for r in res]

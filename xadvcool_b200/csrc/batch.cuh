@@ -26,7 +26,7 @@ struct BatchDesign {
   const void* Q[2];
   const uint32_t* link;
   const float* qsrc;
-  const float* u_in;
+  float* u_in;  // inlet velocity (device): the constant-power pump updates it
   float *rho, *ux, *uy, *uz, *T;
   uint32_t ncell, tiles, stat_tiles, row_base;
   long long min_steps;
@@ -113,6 +113,8 @@ struct BatchRun {
   int stats_every;
   double tol_ke, tol_T;
   unsigned long long spin_limit;
+  int constant_power;  // pump_mode == "constant_power" (src/simulation.py:139-146)
+  double target_power;
 };
 
 template <typename S>
@@ -216,6 +218,17 @@ __global__ void __launch_bounds__(256, XAC_BATCH_MIN_BLOCKS) batch_persistent_ke
           d.prev_ke = ke;
           d.prev_max_T = max_T;
           d.prev_Q = Q_out;
+          if (run.constant_power && s1 > 2000) {
+            // src/simulation.py:139-146, the controller of xac_lattice_run on this design's stats
+            double ue = (double)__ldcg(d.u_in);
+            const double rin = st[XAC_ST_C_IN] > 0 ? st[XAC_ST_SUM_RHO_IN] / st[XAC_ST_C_IN] : 1.0;
+            const double rout = st[XAC_ST_C_OUT] > 0 ? st[XAC_ST_SUM_RHO_OUT] / st[XAC_ST_C_OUT] : 1.0;
+            const double dP = (rin - rout) / 3.0;
+            const double pw = dP * (ue * st[XAC_ST_C_IN]);
+            ue = ue + 0.005 * (run.target_power - pw);
+            ue = ue < 0.0001 ? 0.0001 : (ue > 0.15 ? 0.15 : ue);
+            __stcg(d.u_in, (float)ue);
+          }
           for (int j = 0; j < kNStats; ++j) d.last[j] = st[j];
           d.steps = s1;
           if (s1 > d.min_steps && d.d_ke < run.tol_ke && d.dT < run.tol_T && d.dQ < run.tol_T) {

@@ -1113,7 +1113,6 @@ int xac_batch_get_tune(const xac_batch* b, int* block, int* steps_per_launch) {
 int xac_batch_run(xac_batch* b, const xac_run_opts* o, xac_run_result* res, void* stream) {
   XAC_REQUIRE(b && o && res, "xac_batch_run: null pointer");
   XAC_REQUIRE(o->stats_every > 0 && o->max_steps >= 0, "xac_batch_run: bad options");
-  XAC_REQUIRE(!o->constant_power, "xac_batch_run: the constant-power pump is run per lattice (xac_lattice_run)");
   cudaStream_t s = as_stream(stream);
   const int n = (int)b->lats.size();
   b->hD.assign(n, BatchDesign{});
@@ -1166,6 +1165,8 @@ int xac_batch_run(xac_batch* b, const xac_run_opts* o, xac_run_result* res, void
   run.tol_ke = o->tol_ke;
   run.tol_T = o->tol_T;
   run.spin_limit = 1ull << 27;  // about 10 s of polling before a wait reports XAC_ETIMEOUT
+  run.constant_power = o->constant_power;
+  run.target_power = o->target_power;
   long long done = 0;
   while (done < o->max_steps && !b->hC->all_done) {
     const long long left = o->max_steps - done;
@@ -1186,6 +1187,9 @@ int xac_batch_run(xac_batch* b, const xac_run_opts* o, xac_run_result* res, void
     done = b->hC->step;
   }
   XAC_CUDA(cudaMemcpyAsync(b->hD.data(), b->dD, n * sizeof(BatchDesign), cudaMemcpyDeviceToHost, s));
+  std::vector<float> u_fin(n);
+  for (int i = 0; i < n; ++i)  // the inlet velocities the pump left (one small copy per design)
+    XAC_CUDA(cudaMemcpyAsync(&u_fin[i], b->lats[i]->impl.u_in, sizeof(float), cudaMemcpyDeviceToHost, s));
   XAC_CUDA(cudaStreamSynchronize(s));
   for (int i = 0; i < n; ++i) {
     const BatchDesign& d = b->hD[i];
@@ -1199,9 +1203,10 @@ int xac_batch_run(xac_batch* b, const xac_run_opts* o, xac_run_result* res, void
     rr.d_ke = d.d_ke;
     rr.dT_conv = d.dT;
     rr.dQ_conv = d.dQ;
-    rr.u_inlet_final = (double)b->lats[i]->impl.u_in_host;
-    std::memcpy(rr.last_stats, d.last, sizeof(d.last));
     LatticeImpl& L = b->lats[i]->impl;
+    L.u_in_host = u_fin[i];
+    rr.u_inlet_final = (double)u_fin[i];
+    std::memcpy(rr.last_stats, d.last, sizeof(d.last));
     L.step = steps;
     L.cur = (int)(steps & 1);
     L.own_pending = steps == 0;

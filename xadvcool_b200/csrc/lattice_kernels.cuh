@@ -170,7 +170,8 @@ __device__ __forceinline__ void fluid_cell(const uint32_t c, const Acc& P, S* __
 #define XAC_LD_OWN(I) k[I] = Pop<S>::template ld<kLd>(P.own(I), w_of(I));
     XAC_FOR19(XAC_LD_OWN)
 #undef XAC_LD_OWN
-    const float ux_in = __ldg(u_in_ptr);
+    // the batch kernel's pump controller changes the inlet within a launch: read it through L2 there
+    const float ux_in = kLd == 1 ? __ldcg(u_in_ptr) : __ldg(u_in_ptr);
     const float rn = (((((((((k[0] + k[3]) + k[4]) + k[5]) + k[6]) + k[15]) + k[16]) + k[17]) + k[18]) +
                       2.0f * ((((k[2] + k[8]) + k[10]) + k[12]) + k[14])) /
                      (1.0f - ux_in);
