@@ -295,6 +295,31 @@ int xac_conv3d_partial_floats(int N, int D, int H, int W, int Ci, int Co, int ks
 int xac_conv3d_status(int *flags);
 
 /* ========================================================================== *
+ * Design generator on the device: the seeded benchmark families of xadvcool_b200.designs (gyroid_design,
+ * mixed_design) evaluated per cell. No reference counterpart on the device: the reference builds masks with numpy
+ * (src/geometry.py:339-526). The host draws the random parameters and fills the spec.
+ * ========================================================================== */
+#define XAC_DESIGN_STRAIGHT 1   /* p0 = channel width, p1 = channel count (src/geometry.py:385-434) */
+#define XAC_DESIGN_PIN_FIN 2    /* p0 = pin radius, p1 = pitch: two interleaved square lattices of pins */
+#define XAC_DESIGN_GYROID 3     /* p0 = cell size L, p1 = threshold t: solid where the TPMS value > t */
+#define XAC_DESIGN_SCHWARZ_P 4
+#define XAC_DESIGN_SCHWARZ_D 5
+#define XAC_DESIGN_MAX_HOT 8
+typedef struct xac_design_spec {
+    int nx, ny, nz;       /* lattice, reference layout [nx][ny][nz] */
+    int buf;              /* inlet / outlet buffer cells; the core is x in [buf, nx - buf) */
+    int family;           /* XAC_DESIGN_* */
+    int margin;           /* TPMS: core x cells at each end kept fluid */
+    double p0, p1;        /* family parameters (above) */
+    int n_hot;            /* Gaussian hotspots of the z = 0 floor map, <= XAC_DESIGN_MAX_HOT */
+    double background;    /* floor map background (0.2) */
+    double hot[XAC_DESIGN_MAX_HOT][4];  /* cx, cy (core cells), sigma, amplitude */
+} xac_design_spec;
+/* mask_dev: int32 [nx][ny][nz] BC labels with the reference frame; heat_dev: float32 [nx][ny][nz], the floor map
+ * at z = 0 of the core (0 elsewhere). Both DEVICE pointers. */
+int xac_design_build(const xac_design_spec *spec, int32_t *mask_dev, float *heat_dev, void *stream);
+
+/* ========================================================================== *
  * Batch: many designs (uneven lattice sizes, one precision) advanced together by ONE persistent cooperative
  * launch per `steps_per_launch` steps (captured in a CUDA graph where the driver allows it). Each design keeps
  * the convergence test and divergence guard of src/simulation.py:123-156, evaluated on the device; converged

@@ -44,7 +44,8 @@ def test_struct_layout_matches_header(tmp_path):
 int main(void) {{
   printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(xac_desc), offsetof(xac_desc, tau_fluid), offsetof(xac_desc, precision),
          sizeof(xac_scalar_params), sizeof(xac_run_opts), sizeof(xac_run_result));
-  printf("%zu %zu\\n", offsetof(xac_run_result, u_inlet_final), offsetof(xac_run_result, last_stats));
+  printf("%zu %zu %zu %zu %zu\\n", offsetof(xac_run_result, u_inlet_final), offsetof(xac_run_result, last_stats),
+         sizeof(xac_design_spec), offsetof(xac_design_spec, background), offsetof(xac_design_spec, hot));
   return 0;
 }}''')
     exe = tmp_path / "layout"
@@ -53,7 +54,8 @@ int main(void) {{
     got = [int(v) for v in a.split()] + [int(v) for v in b.split()]
     want = [C.sizeof(_capi.Desc), _capi.Desc.tau_fluid.offset, _capi.Desc.precision.offset,
             C.sizeof(_capi.ScalarParams), C.sizeof(_capi.RunOpts), C.sizeof(_capi.RunResult),
-            _capi.RunResult.u_inlet_final.offset, _capi.RunResult.last_stats.offset]
+            _capi.RunResult.u_inlet_final.offset, _capi.RunResult.last_stats.offset, C.sizeof(_capi.DesignSpec),
+            _capi.DesignSpec.background.offset, _capi.DesignSpec.hot.offset]
     assert got == want
 
 

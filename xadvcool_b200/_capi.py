@@ -65,6 +65,17 @@ class RunOpts(C.Structure):
     ]
 
 
+class DesignSpec(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("buf", C.c_int), ("family", C.c_int),
+        ("margin", C.c_int), ("p0", C.c_double), ("p1", C.c_double), ("n_hot", C.c_int),
+        ("background", C.c_double), ("hot", (C.c_double * 4) * 8),
+    ]
+
+
+DESIGN_FAMILIES = {"straight": 1, "pin_fin": 2, "gyroid": 3, "schwarz_p": 4, "schwarz_d": 5}
+
+
 class RunResult(C.Structure):
     _fields_ = [
         ("steps", C.c_longlong), ("converged", C.c_int), ("diverged", C.c_int),
@@ -112,6 +123,7 @@ SIGNATURES = {
     "xac_lattice_load_state": [_vp, _vp, C.c_size_t, _vp],
     "xac_lattice_run": [_vp, C.POINTER(RunOpts), C.POINTER(RunResult), _vp],
     "xac_lattice_validate": [_vp, _vp, _vp],
+    "xac_design_build": [C.POINTER(DesignSpec), _vp, _vp, _vp],
     "xac_conv3d_forward": [_vp, _i, _i, _i, _i, _i, _vp, _vp, _i, _i, _i, _vp, _vp, _vp],
     "xac_conv3d_weight_grad": [_vp, _i, _i, _i, _i, _i, _vp, _i, _i, _vp, _vp, _vp, _vp],
     "xac_conv3d_partial_floats": [_i, _i, _i, _i, _i, _i, _i, C.POINTER(C.c_longlong)],

@@ -30,6 +30,7 @@ UNITS = [
     ("step_bf16.cu", ["--fmad=false"]),
     ("stats_noalloc.cu", ["--fmad=false"]),
     ("conv3d.cu", []),
+    ("designs.cu", ["--fmad=false"]),
 ]
 
 

@@ -253,33 +253,104 @@ def straight_fin_plate(nx=64, ny=32, nz=16, fins=((4, 6), (9, 11), (14, 16), (19
     return _frame(mask)
 
 
-def seeded_hotspot_map(rng: np.random.Generator, nx: int, ny: int) -> np.ndarray:
-    """0.2 background plus K ~ U{1..4} Gaussian hotspots, sigma ~ U[4,12] cells, amplitude ~ U[0.5,1]."""
-    hm = np.full((nx, ny), 0.2, dtype=np.float64)
-    xx, yy = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+def draw_hotspots(rng: np.random.Generator, nx: int, ny: int):
+    """K ~ U{1..4} Gaussian hotspots (cx, cy, sigma ~ U[4,12] cells, amplitude ~ U[0.5,1])."""
+    out = []
     for _ in range(int(rng.integers(1, 5))):
         cx, cy = rng.uniform(0, nx), rng.uniform(0, ny)
         sigma = rng.uniform(4.0, 12.0)
         amp = rng.uniform(0.5, 1.0)
+        out.append((cx, cy, sigma, amp))
+    return out
+
+
+def hotspot_map(hot, nx: int, ny: int) -> np.ndarray:
+    """0.2 background plus the given Gaussian hotspots, evaluated in float64, stored as float32."""
+    hm = np.full((nx, ny), 0.2, dtype=np.float64)
+    xx, yy = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    for cx, cy, sigma, amp in hot:
         hm += amp * np.exp(-((xx - cx) ** 2 + (yy - cy) ** 2) / (2.0 * sigma ** 2))
     return hm.astype(np.float32)
+
+
+def seeded_hotspot_map(rng: np.random.Generator, nx: int, ny: int) -> np.ndarray:
+    """0.2 background plus K ~ U{1..4} Gaussian hotspots, sigma ~ U[4,12] cells, amplitude ~ U[0.5,1]."""
+    return hotspot_map(draw_hotspots(rng, nx, ny), nx, ny)
+
+
+def gyroid_spec(seed: int, nx=148, ny=128, nz=32, buf=10) -> dict:
+    """The random draws of gyroid_design: L ~ U{12..24}, t ~ U[-0.4, 0.4], u_in ~ U[0.02, 0.08], then the
+    hotspot map's draws. The returned spec also drives the device builder (xadvcool_b200.device_designs)."""
+    rng = np.random.default_rng(seed)
+    L = int(rng.integers(12, 25))
+    t = float(rng.uniform(-0.4, 0.4))
+    u_in = float(rng.uniform(0.02, 0.08))
+    core = nx - 2 * buf
+    return {"family": "gyroid", "shape": (nx, ny, nz), "buf": buf, "L": L, "t": t, "margin": 0, "u_in": u_in,
+            "hot": draw_hotspots(rng, core, ny), "seed": seed}
+
+
+def mixed_spec(seed: int, family: str | None = None) -> dict:
+    """The random draws of mixed_design, in its order."""
+    rng = np.random.default_rng(10_000 + seed)
+    fam = family or FAMILIES[seed % len(FAMILIES)]
+    nx = int(rng.choice([96, 128, 148, 192]))
+    ny = int(rng.choice([64, 96, 128]))
+    nz = int(rng.choice([16, 32, 48]))
+    buf = 10
+    core = nx - 2 * buf
+    spec = {"family": fam, "shape": (nx, ny, nz), "buf": buf, "seed": seed, "margin": 0}
+    if fam == "straight":
+        n = int(rng.integers(4, 13))
+        spec.update(n=n, width=max(2, (ny - 2) // (2 * n)))
+    elif fam == "pin_fin":
+        radius = int(rng.integers(2, 6))
+        spec.update(radius=radius, pitch=int(rng.integers(max(8, 2 * radius + 2), 17)))
+    else:
+        spec.update(L=int(rng.integers(12, 25)), t=float(rng.uniform(-0.3, 0.3)), margin=5)
+    spec["u_in"] = float(rng.uniform(0.02, 0.05))
+    spec["hot"] = draw_hotspots(rng, core, ny)
+    return spec
+
+
+_TPMS_KIND = {"gyroid": 3, "schwarz_p": 4, "schwarz_d": 5}
+
+
+def build_from_spec(spec: dict):
+    """Host evaluation of a spec -> (mask int32 [nx][ny][nz], heat source float32 [nx][ny][nz])."""
+    nx, ny, nz = spec["shape"]
+    buf = spec["buf"]
+    core = nx - 2 * buf
+    fam = spec["family"]
+    solid = np.zeros((core, ny, nz), dtype=bool)
+    if fam == "straight":
+        _straight_channels(solid, spec["width"], spec["n"])
+    elif fam == "pin_fin":
+        radius, pitch = spec["radius"], spec["pitch"]
+        X, Y = np.meshgrid(np.arange(core), np.arange(ny), indexing="ij")
+        da = ((X % pitch) - pitch / 2) ** 2 + ((Y % pitch) - pitch / 2) ** 2
+        db = (((X - pitch / 2) % pitch) - pitch / 2) ** 2 + (((Y - pitch / 2) % pitch) - pitch / 2) ** 2
+        solid[:, :, :] = (np.minimum(da, db) < radius ** 2)[:, :, None]
+    else:
+        solid = tpms_field(_TPMS_KIND[fam], (core, ny, nz), float(spec["L"])) > spec["t"]
+        m = spec.get("margin", 0)
+        if m:
+            solid[:m] = False
+            solid[-m:] = False
+    mask = np.full((nx, ny, nz), BC_FLUID, dtype=np.int32)
+    mask[buf:buf + core][solid] = BC_SOLID
+    mask = _frame(mask)
+    hs = floor_heat_source((nx, ny, nz), hotspot_map(spec["hot"], core, ny), buf=buf)
+    return mask, hs
 
 
 def gyroid_design(seed: int, nx=148, ny=128, nz=32, buf=10):
     """148x128x32 gyroid: solid where sin(kx)cos(ky)+sin(ky)cos(kz)+sin(kz)cos(kx) > t, k = 2pi/L,
     L ~ U{12..24}, t ~ U[-0.4, 0.4], in the core x in [buf, nx-buf), plus the reference frame
     (4-cell base plate, walls, inlet/outlet). Returns (mask, heat_source, u_inlet, info)."""
-    rng = np.random.default_rng(seed)
-    L = int(rng.integers(12, 25))
-    t = float(rng.uniform(-0.4, 0.4))
-    u_in = float(rng.uniform(0.02, 0.08))
-    core = nx - 2 * buf
-    solid = tpms_field(3, (core, ny, nz), float(L)) > t
-    mask = np.full((nx, ny, nz), BC_FLUID, dtype=np.int32)
-    mask[buf:buf + core][solid] = BC_SOLID
-    mask = _frame(mask)
-    hs = floor_heat_source((nx, ny, nz), seeded_hotspot_map(rng, core, ny), buf=buf)
-    return mask, hs, u_in, {"L": L, "t": t, "u_in": u_in, "seed": seed}
+    spec = gyroid_spec(seed, nx, ny, nz, buf)
+    mask, hs = build_from_spec(spec)
+    return mask, hs, spec["u_in"], {"L": spec["L"], "t": spec["t"], "u_in": spec["u_in"], "seed": seed}
 
 
 FAMILIES = ("straight", "pin_fin", "gyroid", "schwarz_p", "schwarz_d")
@@ -289,40 +360,10 @@ def mixed_design(seed: int, family: str | None = None):
     """One uneven-size design of the five families with x in {96,128,148,192}, y in {64,96,128},
     z in {16,32,48}: straight channels (n = 4..12), staggered pin fins (radius 2..5, pitch 8..16), gyroid,
     Schwarz P (cos+cos+cos > t) and Schwarz D. Returns (mask, heat_source, u_inlet, info)."""
-    rng = np.random.default_rng(10_000 + seed)
-    fam = family or FAMILIES[seed % len(FAMILIES)]
-    nx = int(rng.choice([96, 128, 148, 192]))
-    ny = int(rng.choice([64, 96, 128]))
-    nz = int(rng.choice([16, 32, 48]))
-    buf = 10
-    core = nx - 2 * buf
-    solid = np.zeros((core, ny, nz), dtype=bool)
-    info = {"family": fam, "shape": (nx, ny, nz), "seed": seed}
-    if fam == "straight":
-        n = int(rng.integers(4, 13))
-        width = max(2, (ny - 2) // (2 * n))
-        _straight_channels(solid, width, n)
-        info.update(n=n, width=width)
-    elif fam == "pin_fin":
-        radius = int(rng.integers(2, 6))
-        pitch = int(rng.integers(max(8, 2 * radius + 2), 17))
-        X, Y = np.meshgrid(np.arange(core), np.arange(ny), indexing="ij")
-        da = ((X % pitch) - pitch / 2) ** 2 + ((Y % pitch) - pitch / 2) ** 2
-        db = (((X - pitch / 2) % pitch) - pitch / 2) ** 2 + (((Y - pitch / 2) % pitch) - pitch / 2) ** 2
-        solid[:, :, :] = (np.minimum(da, db) < radius ** 2)[:, :, None]
-        info.update(radius=radius, pitch=pitch)
-    else:
-        kind = {"gyroid": 3, "schwarz_p": 4, "schwarz_d": 5}[fam]
-        L = int(rng.integers(12, 25))
-        t = float(rng.uniform(-0.3, 0.3))
-        solid = tpms_field(kind, (core, ny, nz), float(L)) > t
-        solid[:5] = False
-        solid[-5:] = False
-        info.update(L=L, t=t)
-    mask = np.full((nx, ny, nz), BC_FLUID, dtype=np.int32)
-    mask[buf:buf + core][solid] = BC_SOLID
-    mask = _frame(mask)
-    u_in = float(rng.uniform(0.02, 0.05))
-    hs = floor_heat_source((nx, ny, nz), seeded_hotspot_map(rng, core, ny), buf=buf)
-    info["u_in"] = u_in
-    return mask, hs, u_in, info
+    spec = mixed_spec(seed, family)
+    mask, hs = build_from_spec(spec)
+    info = {"family": spec["family"], "shape": spec["shape"], "seed": seed, "u_in": spec["u_in"]}
+    for k in ("n", "width", "radius", "pitch", "L", "t"):
+        if k in spec:
+            info[k] = spec[k]
+    return mask, hs, spec["u_in"], info
