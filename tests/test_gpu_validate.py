@@ -63,7 +63,8 @@ def test_dataset_writer_from_a_lattice(cuda, tmp_path):
     row = w.add_lattice("g2", lat, design, res, elapsed_s=0.1, buf=6)
     w.close()
     sc = lat.scalars(buf=6, core_nx=36, core_ny=24)
-    assert row["Nu"] == sc["Nu"] and row["sim_steps"] == 300 and row["grid_cells"] == mask.size
+    assert row["Nu"] == sc["Nu"] and row["sim_steps"] == res["steps"] and row["grid_cells"] == mask.size
+    assert row["converged"] == res["converged"]
     data, attrs = D.load_sample(tmp_path / "samples" / "g2.npz")
     rho, u, T = (t.cpu().numpy() for t in lat.fields())
     assert np.array_equal(data["temperature"], T) and np.array_equal(data["velocity"], u)
