@@ -8,10 +8,10 @@
 //   data grad the forward kernel applied to d_out with the flipped, transposed weights
 //             w'[26 - tap][ci][co] = w[tap][co][ci] (the adjoint of a zero-padded convolution).
 //   weight grad dw[tap][co][ci] = sum_v d_out[v][co] * in[v + off(tap)][ci]
-//             GEMM M = Co, N = Ci, K = voxels, split over voxel chunks; partials reduced in a fixed order.
+//             GEMM M = taps * Co, N = Ci, K = voxels on tcgen05, split over voxel chunks; partials reduced in a
+//             fixed order.
 //
-// The weight gradient uses mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 tiles. Ci and Co must be multiples
-// of 16 (the model pads its 3 input channels and 5 output channels to 16).
+// Ci and Co must be multiples of 16 (the model pads its 3 input channels and 5 output channels to 16).
 #include <cuda_bf16.h>
 
 #include <cstdint>
@@ -27,13 +27,6 @@ struct ConvShape {
   int ksize;  // 1 or 3
 };
 
-__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
 
 
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
@@ -291,66 +284,143 @@ __global__ void __launch_bounds__(128, 1) conv_fwd_tc_kernel(const __nv_bfloat16
   }
 }
 
-// ---- weight grad ------------------------------------------------------------------------------------
-// Block: one tap, one 16 (co) x 16 (ci) tile, one chunk of voxels (the GEMM's K). 4 warps split the chunk's k16
-// steps; their partials are added in warp order through shared memory. Output: partial[chunk][tap][co][ci].
-constexpr int kWgChunk = 2048;
-__global__ void __launch_bounds__(128) conv_wgrad_kernel(const __nv_bfloat16* __restrict__ in,
-                                                         const __nv_bfloat16* __restrict__ dout, ConvShape s,
-                                                         float* __restrict__ partial) {
+// ---- weight grad on the tensor cores (tcgen05) --------------------------------------------------------
+// With u = v + off(tap): dw[tap][co][ci] = sum_u d_out[u - off(tap)][co] * in[u][ci], a GEMM with rows
+// m = tap * Co + co (M = taps * Co), columns ci (N = Ci) and K = voxels. A CTA computes 128 rows x Ci columns in
+// tensor memory over one chunk of kWgKC voxels (split K), 64 voxels per stage:
+//   A (MN-major): A[m][u] = d_out[u - off(tap)][co], zero where u - off(tap) leaves the volume;
+//   B (MN-major): B[u][ci] = in[u][ci].
+// Shared-memory layout of both: core matrices of 8 M (or N) values x 8 voxels, 128 contiguous bytes each (one
+// voxel's 8 values per 16-byte row); M/N groups 128 bytes apart (stride byte offset), 8-voxel groups one group
+// row apart (leading byte offset). The chunk's partial goes to partial[chunk][m][ci]; the chunks are added in
+// order by wgrad_reduce_kernel (deterministic). Bounded waits as in the forward kernel.
+constexpr int kWgKC = 4096;  // voxels per CTA
+constexpr int kWgBK = 64;    // voxels per stage
+
+__global__ void __launch_bounds__(128, 1) conv_wgrad_tc_kernel(const __nv_bfloat16* __restrict__ in,
+                                                               const __nv_bfloat16* __restrict__ dout, ConvShape s,
+                                                               uint32_t ncols, float* __restrict__ partial) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bars[2 * kTcStages + 1];
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int Ci = s.Ci, Co = s.Co, taps = s.ksize == 3 ? 27 : 1, Mtot = taps * Co;
   const long long V = (long long)s.N * s.D * s.H * s.W;
-  const int tap = blockIdx.y, chunk = blockIdx.x;
-  const int ci_tiles = s.Ci / 16;
-  const int co0 = (blockIdx.z / ci_tiles) * 16, ci0 = (blockIdx.z % ci_tiles) * 16;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int r = lane >> 2, cq = (lane & 3) * 2;
-  const int dz = s.ksize == 3 ? tap / 9 - 1 : 0, dy = s.ksize == 3 ? (tap / 3) % 3 - 1 : 0,
-            dx = s.ksize == 3 ? tap % 3 - 1 : 0;
-  float acc[2][4] = {{0.0f, 0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f, 0.0f}};
-  auto pack = [](float lo, float hi) {
-    __nv_bfloat162 p = __floats2bfloat162_rn(lo, hi);
-    return *reinterpret_cast<uint32_t*>(&p);
-  };
-  const long long vbeg = (long long)chunk * kWgChunk;
-  for (long long k0 = vbeg + warp * 16; k0 < vbeg + kWgChunk && k0 < V; k0 += 64) {
-    // A = d_out^T: rows co0 + r (+8), cols voxels k0 + cq (+1), +8 (+9)
-    const long long vk[4] = {k0 + cq, k0 + cq + 1, k0 + cq + 8, k0 + cq + 9};
-    float dv[2][4];
-    long long nv[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const bool ok = vk[q] < V;
-      dv[0][q] = ok ? __bfloat162float(dout[vk[q] * s.Co + co0 + r]) : 0.0f;
-      dv[1][q] = ok ? __bfloat162float(dout[vk[q] * s.Co + co0 + r + 8]) : 0.0f;
-      nv[q] = ok ? neighbour(decode(vk[q], s), dz, dy, dx, s) : -1;
+  const int m0 = blockIdx.x * kTcM;
+  const long long u_begin = (long long)blockIdx.y * kWgKC;
+  const long long u_left = V - u_begin;
+  const int KT = (int)(((u_left < kWgKC ? u_left : kWgKC) + kWgBK - 1) / kWgBK);
+  const uint32_t a_bytes = kTcM * kWgBK * 2, b_bytes = (uint32_t)kWgBK * Ci * 2, stage_bytes = a_bytes + b_bytes;
+  const uint32_t a_lbo = (kTcM / 8) * 128u, b_lbo = (uint32_t)(Ci / 8) * 128u;
+  const uint32_t sbase = smem_addr(smem);
+  const uint32_t bar0 = smem_addr(bars);
+  auto full = [&](int st) { return bar0 + 8u * st; };
+  auto empty = [&](int st) { return bar0 + 8u * (kTcStages + st); };
+  const uint32_t done_bar = bar0 + 8u * (2 * kTcStages);
+  if (tid == 0) {
+    for (int st = 0; st < kTcStages; ++st) {
+      mbar_init(full(st), 128);
+      mbar_init(empty(st), 1);
     }
-    const uint32_t a[4] = {pack(dv[0][0], dv[0][1]), pack(dv[1][0], dv[1][1]), pack(dv[0][2], dv[0][3]),
-                           pack(dv[1][2], dv[1][3])};
-    // B = shifted input: rows voxels vk, cols ci0 + j*8 + r
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      const int ci = ci0 + j * 8 + r;
-      float bv[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) bv[q] = nv[q] >= 0 ? __bfloat162float(in[nv[q] * s.Ci + ci]) : 0.0f;
-      const uint32_t b[2] = {pack(bv[0], bv[1]), pack(bv[2], bv[3])};
-      mma_bf16_16816(acc[j], a, b);
-    }
+    mbar_init(done_bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  __shared__ float red[4][16][16];
-#pragma unroll
-  for (int j = 0; j < 2; ++j) {
-    const int ci = j * 8 + cq;
-    red[warp][r][ci] = acc[j][0];
-    red[warp][r][ci + 1] = acc[j][1];
-    red[warp][r + 8][ci] = acc[j][2];
-    red[warp][r + 8][ci + 1] = acc[j][3];
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
+                 "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
+  tc_fence_before();
   __syncthreads();
-  for (int e = threadIdx.x; e < 256; e += blockDim.x) {
-    const int row = e >> 4, col = e & 15;
-    const float v = ((red[0][row][col] + red[1][row][col]) + red[2][row][col]) + red[3][row][col];
-    partial[(((long long)chunk * gridDim.y + tap) * s.Co + co0 + row) * s.Ci + ci0 + col] = v;
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  const uint32_t idesc = tc_idesc(Ci) | (1u << 15) | (1u << 16);  // A and B MN-major
+  const int ul = tid & 63, g0 = tid >> 6;  // this thread's voxel in a stage, and first M / N group
+  const int kg = ul >> 3, krow = ul & 7;
+
+  auto load_stage = [&](int k, int st) {
+    const uint32_t a_st = sbase + (uint32_t)st * stage_bytes, b_st = a_st + a_bytes;
+    const long long u = u_begin + (long long)k * kWgBK + ul;
+    const bool uok = u < V && k * kWgBK + ul < kWgKC;
+    const VoxelCoord cu = decode(uok ? u : 0, s);
+    for (int j = 0; j < 8; ++j) {
+      const int mg = g0 + 2 * j, m = m0 + mg * 8;
+      long long src = -1;
+      int co = 0;
+      if (uok && m < Mtot) {
+        const int tap = m / Co;
+        co = m - tap * Co;
+        const int dz = s.ksize == 3 ? tap / 9 - 1 : 0, dy = s.ksize == 3 ? (tap / 3) % 3 - 1 : 0,
+                  dx = s.ksize == 3 ? tap % 3 - 1 : 0;
+        src = neighbour(cu, -dz, -dy, -dx, s);
+      }
+      cp_async16(a_st + ((uint32_t)(kg * (kTcM / 8) + mg) * 8u + krow) * 16u,
+                 src >= 0 ? (const void*)(dout + src * Co + co) : (const void*)dout, src >= 0 ? 16u : 0u);
+    }
+    for (int ng = g0; ng < Ci / 8; ng += 2)
+      cp_async16(b_st + ((uint32_t)(kg * (Ci / 8) + ng) * 8u + krow) * 16u,
+                 uok ? (const void*)(in + u * Ci + ng * 8) : (const void*)in, uok ? 16u : 0u);
+  };
+  auto mma_stage = [&](int k, int st) {
+    const uint32_t a_st = sbase + (uint32_t)st * stage_bytes, b_st = a_st + a_bytes;
+    for (int q = 0; q < kWgBK / 16; ++q) {
+      const uint64_t ad = smem_desc(a_st + (uint32_t)(2 * q) * a_lbo, a_lbo, 128u);
+      const uint64_t bd = smem_desc(b_st + (uint32_t)(2 * q) * b_lbo, b_lbo, 128u);
+      tc_mma(tmem, ad, bd, idesc, (k > 0 || q > 0) ? 1u : 0u);
+    }
+    tc_commit(empty(st));
+  };
+
+  for (int k = 0; k < KT + kTcStages - 1; ++k) {
+    if (k < KT) {
+      const int st = k % kTcStages;
+      if (k >= kTcStages && !mbar_wait(empty(st), ((k / kTcStages) - 1) & 1)) abort_flag = 1;
+      if (abort_flag) break;
+      load_stage(k, st);
+    }
+    cp_async_commit();
+    const int kc = k - (kTcStages - 1);
+    if (kc >= 0) {
+      cp_async_wait<kTcStages - 1>();
+      fence_proxy_async();
+      mbar_arrive(full(kc % kTcStages));
+      if (warp == 0) {
+        if (mbar_wait(full(kc % kTcStages), (kc / kTcStages) & 1)) {
+          tc_fence_after();
+          if (lane == 0) mma_stage(kc, kc % kTcStages);
+        } else {
+          abort_flag = 1;
+        }
+        __syncwarp();
+      }
+    }
+    if (abort_flag) break;
+  }
+  cp_async_wait<0>();
+  if (tid == 0) tc_commit(done_bar);
+  const int drained = mbar_wait(done_bar, 0) ? 1 : 0;
+  const bool ok = __syncthreads_and(drained) && !abort_flag;
+  tc_fence_after();
+  if (ok) {
+    const int m = m0 + warp * 32 + lane;
+    float* dst = partial + ((long long)blockIdx.y * Mtot + m) * Ci;
+    for (int c0 = 0; c0 < Ci; c0 += 16) {
+      float x[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, x);
+      if (m < Mtot) {
+        float4* d4 = reinterpret_cast<float4*>(dst + c0);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) d4[i] = make_float4(x[4 * i], x[4 * i + 1], x[4 * i + 2], x[4 * i + 3]);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
   }
 }
 
@@ -447,10 +517,20 @@ int xac_conv3d_weight_grad(const void* in, int N, int D, int H, int W, int Ci, c
   XAC_REQUIRE(in && dout && partial && dw, "xac_conv3d_weight_grad: null pointer");
   const long long V = (long long)N * D * H * W;
   const int taps = ksize == 3 ? 27 : 1;
-  const int nchunks = (int)((V + kWgChunk - 1) / kWgChunk);
-  dim3 grid(nchunks, taps, (Co / 16) * (Ci / 16));
+  const int nchunks = (int)((V + kWgKC - 1) / kWgKC);
+  uint32_t ncols = 32;
+  while ((int)ncols < Ci) ncols <<= 1;
+  static bool attr_set = false;
+  if (!attr_set) {
+    XAC_CUDA(cudaFuncSetAttribute(conv_wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)((size_t)kTcStages * (kTcM * kWgBK + kWgBK * 256) * 2)));
+    attr_set = true;
+  }
+  const dim3 grid((unsigned)((taps * Co + kTcM - 1) / kTcM), (unsigned)nchunks);
+  const size_t smem = (size_t)kTcStages * (kTcM * kWgBK + kWgBK * Ci) * 2;
   cudaStream_t st = as_stream(stream);
-  conv_wgrad_kernel<<<grid, 128, 0, st>>>((const __nv_bfloat16*)in, (const __nv_bfloat16*)dout, s, partial);
+  conv_wgrad_tc_kernel<<<grid, 128, smem, st>>>((const __nv_bfloat16*)in, (const __nv_bfloat16*)dout, s, ncols,
+                                                 partial);
   const long long per_chunk = (long long)taps * Co * Ci;
   wgrad_reduce_kernel<<<(unsigned)((per_chunk + 255) / 256), 256, 0, st>>>(partial, nchunks, per_chunk, dw);
   if (db) {
@@ -474,7 +554,7 @@ int xac_conv3d_status(int* flags) {
 int xac_conv3d_partial_floats(int N, int D, int H, int W, int Ci, int Co, int ksize, long long* count) {
   XAC_REQUIRE(count, "xac_conv3d_partial_floats: null pointer");
   const long long V = (long long)N * D * H * W;
-  const long long w = ((V + kWgChunk - 1) / kWgChunk) * (ksize == 3 ? 27 : 1) * (long long)Co * Ci;
+  const long long w = ((V + kWgKC - 1) / kWgKC) * (ksize == 3 ? 27 : 1) * (long long)Co * Ci;
   const long long b = (long long)kBiasBlocks * Co;
   *count = w > b ? w : b;
   return XAC_OK;
