@@ -203,8 +203,10 @@ int xac_lattice_set_inlet(xac_lattice *lat, double u_inlet, void *stream);
 int xac_lattice_get_inlet(xac_lattice *lat, double *u_inlet, void *stream);
 int xac_lattice_steps_done(const xac_lattice *lat, long long *steps);
 /* Launch shape of the fused step kernel: threads per block (64, 128, 256) and the visiting order:
- * variant must be 0 (one thread per row position, in memory order). Results do not depend on the block size (every
- * cell runs the same arithmetic); xadvcool_b200.autotune picks it. */
+ * variant 0 = one thread per row position, in memory order; variant 1 = one block per row whose thermal input is
+ * staged in shared memory by bulk copies while the fluid lattice runs (row lengths 64..256; other lengths run
+ * variant 0). Results do not depend on the shape (every cell runs the same arithmetic); xadvcool_b200.autotune
+ * picks it. */
 int xac_lattice_tune(xac_lattice *lat, int block, int variant);
 int xac_lattice_get_tune(const xac_lattice *lat, int *block, int *variant);
 /* Inputs of generate_dataset.py:80 compute_macroscopic_metrics that are not fields. */

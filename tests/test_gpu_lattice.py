@@ -201,35 +201,40 @@ def test_16bit_storage_error_vs_fp64_oracle(precision, tol_u, tol_T, cuda):
 @pytest.mark.parametrize("precision", ["fp32", "fp16", "bf16"])
 @pytest.mark.parametrize("block", [64, 128, 256])
 def test_launch_shapes_give_identical_bits(precision, block, cuda):
-    """Every block size, on a lattice whose row length (48 -> pitch 64) has a compile-time instantiation and on one
-    (nx = 300) that takes the runtime-pitch kernel: same bits as the default shape, and the oracle's."""
+    """Every block size and both visiting orders (the staged one takes its block size from the row) on a lattice
+    with a compile-time row length (48 -> pitch 64): same bits as the default shape, and the oracle's."""
     mask, hs, u_in, _ = designs.gyroid_design(3, nx=48, ny=20, nz=12)
     kw = dict(heat_source=hs, tau_fluid=0.56, u_inlet_val=u_in, heat_power=0.05, precision=precision)
     out = {}
-    for key, b in (("default", 128), ("tuned", block)):
+    for key, b, v in (("default", 128, 0), ("tuned", block, 0), ("staged", block, 1)):
         lat = Lattice(mask, **kw)
-        lat.tune(b, 0)
-        assert lat.get_tune() == (b, 0)
+        lat.tune(b, v)
+        assert lat.get_tune() == (b, v)
         lat.step(37)
         out[key] = [t.cpu().numpy() for t in lat.fields()] + [lat.stats()]
         lat.close()
-    for a, b in zip(out["default"], out["tuned"]):
-        assert np.array_equal(a, b)
+    for key in ("tuned", "staged"):
+        for a, b in zip(out["default"], out[key]):
+            assert np.array_equal(a, b)
     if precision == "fp32":
         ref = oracle_fields(mask, 37, hs=hs, tau_fluid=0.56, u_inlet_val=u_in, heat_power=0.05)
         assert_exact(ref, *out["tuned"][:3])
+        assert_exact(ref, *out["staged"][:3])
 
 
-@pytest.mark.parametrize("nx", [20, 33, 100, 300])
-def test_row_lengths_match_oracle(nx, cuda):
-    """Row lengths 32, 64, 128 (compile-time) and 320 (runtime pitch), ragged x padding: bit-exact FP32."""
+@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("nx", [20, 33, 100, 150, 300])
+def test_row_lengths_match_oracle(nx, variant, cuda):
+    """Row lengths 32, 64, 128, 160 (compile-time) and 320 (runtime pitch), ragged x padding, both visiting orders
+    (the staged one falls back to one thread per row position below 64 and above 256): bit-exact FP32."""
     mask, hs, u_in, _ = designs.gyroid_design(5, nx=nx, ny=9, nz=7, buf=4)
-    kw = dict(heat_source=hs, tau_fluid=0.57, u_inlet_val=u_in, heat_power=0.05)
+    kw = dict(heat_source=hs, tau_fluid=0.57, u_inlet_val=min(u_in, 0.04), heat_power=0.05)
     lat = Lattice(mask, **kw)
+    lat.tune(128, variant)
     lat.step(23)
     got = [t.cpu().numpy() for t in lat.fields()]
     lat.close()
-    ref = oracle_fields(mask, 23, hs=hs, tau_fluid=0.57, u_inlet_val=u_in, heat_power=0.05)
+    ref = oracle_fields(mask, 23, hs=hs, tau_fluid=0.57, u_inlet_val=min(u_in, 0.04), heat_power=0.05)
     assert_exact(ref, *got)
 
 
@@ -238,7 +243,7 @@ def test_tune_rejects_bad_shapes(cuda):
     with pytest.raises(Exception):
         lat.tune(96, 0)
     with pytest.raises(Exception):
-        lat.tune(128, 1)
+        lat.tune(128, 2)
 
 
 def test_autotune_picks_a_valid_shape_without_touching_results(cuda, tmp_path, monkeypatch):

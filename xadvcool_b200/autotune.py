@@ -15,7 +15,7 @@ import numpy as np
 import torch
 
 BLOCKS = (64, 128, 256)
-VARIANTS = (0,)  # one visiting order (row positions in memory order)
+VARIANTS = (0, 1)  # 0: one thread per row position; 1: thermal rows staged in shared memory (block = row)
 
 
 def _cache_path() -> Path:
@@ -78,8 +78,8 @@ def autotune(mask, *, heat_source=None, precision="fp32", device="cuda", steps=1
     table = {}
     with Lattice(mask, precision=precision, device=dev, **kw) as scratch:
         scratch.step(2)
-        for b in BLOCKS:
-            for v in VARIANTS:
+        for v in VARIANTS:
+            for b in (BLOCKS if v == 0 else BLOCKS[:1]):  # variant 1 launches one block per row: no block size
                 table[f"{b}x{v}"] = round(time_config(scratch, b, v, steps=steps), 3)
     best = min(table, key=table.get)
     b, v = (int(t) for t in best.split("x"))

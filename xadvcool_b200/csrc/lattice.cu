@@ -173,7 +173,8 @@ struct LatticeImpl {
   float relax[5] = {1.0f, 1.0f, 1.0f, 0.5f, 0.5f};  // omega_f, omega_tf, omega_ts, srcf_f, srcf_s (device-computed)
   float u_in_host = 0.0f;
   int tune_block = 128;  // threads per block of the step kernel
-  int tune_variant = 0;  // one visiting order (row positions in memory order); kept for the ABI
+  int tune_variant = 0;  // 0: one thread per row position; 1: thermal rows staged in shared memory
+  unsigned* status = nullptr;  // device word set by a step kernel whose bounded wait ran out
 
   void* P[2] = {nullptr, nullptr};
   void* Qb[2] = {nullptr, nullptr};
@@ -218,6 +219,7 @@ struct LatticeImpl {
     p.omega_ts = relax[2];
     p.srcf_f = relax[3];
     p.srcf_s = relax[4];
+    p.status = status;
     return p;
   }
 
@@ -227,6 +229,7 @@ struct LatticeImpl {
     cudaFree(type);
     cudaFree(link);
     cudaFree(qsrc);
+    cudaFree(status);
     cudaFree(u_in);
     cudaFree(rho);
     cudaFree(ux);
@@ -246,7 +249,7 @@ struct LatticeImpl {
     S* Pout = (S*)P[cur ^ 1];
     const S* Qin = (const S*)Qb[cur];
     S* Qout = (S*)Qb[cur ^ 1];
-    StepLaunch a{Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux, uy, uz, T, p, tune_block, macro, own, s};
+    StepLaunch a{Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux, uy, uz, T, p, tune_block, tune_variant, macro, own, s};
     launch_coupled_step<S>(a);
     cur ^= 1;
     return XAC_OK;
@@ -526,6 +529,8 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
   if ((r = dmalloc(&L.link, n, "alloc link")) != XAC_OK) return r;
   if ((r = dmalloc(&L.qsrc, n, "alloc qsrc")) != XAC_OK) return r;
   if ((r = dmalloc(&L.u_in, 1, "alloc u_in")) != XAC_OK) return r;
+  if ((r = dmalloc(&L.status, 1, "alloc status")) != XAC_OK) return r;
+  XAC_CUDA(cudaMemsetAsync(L.status, 0, sizeof(unsigned), s));
   for (float** f : {&L.rho, &L.ux, &L.uy, &L.uz, &L.T})
     if ((r = dmalloc(f, n, "alloc fields")) != XAC_OK) return r;
   L.red_blocks = reduction_blocks(n);
@@ -636,6 +641,15 @@ int xac_lattice_stats(xac_lattice* lat, double* out_host, void* stream) {
   r = run_stats(L.view(), L.rows, L.red_out, L.host_out, s);
   if (r != XAC_OK) return r;
   std::memcpy(out_host, L.host_out, kNStats * sizeof(double));
+  if (L.tune_variant == 1) {  // the staged kernel's bounded wait reports here
+    unsigned st = 0;
+    XAC_CUDA(cudaMemcpyAsync(&st, L.status, sizeof(st), cudaMemcpyDeviceToHost, s));
+    XAC_CUDA(cudaStreamSynchronize(s));
+    if (st) {
+      set_error("xac_lattice_stats: a staged step kernel gave up waiting for its copies (status %u)", st);
+      return XAC_ETIMEOUT;
+    }
+  }
   return XAC_OK;
 }
 
@@ -672,7 +686,7 @@ int xac_lattice_tune(xac_lattice* lat, int block, int variant) {
   XAC_REQUIRE(lat, "xac_lattice_tune: null lattice");
   XAC_REQUIRE(block == 64 || block == 128 || block == 256, "xac_lattice_tune: block must be 64, 128 or 256 (got %d)",
               block);
-  XAC_REQUIRE(variant == 0, "xac_lattice_tune: variant must be 0 (got %d)", variant);
+  XAC_REQUIRE(variant == 0 || variant == 1, "xac_lattice_tune: variant must be 0 or 1 (got %d)", variant);
   LatticeImpl& L = lat->impl;
   std::lock_guard<std::mutex> g(L.mu);
   if (L.tune_block != block || L.tune_variant != variant) {

@@ -113,6 +113,7 @@ struct StepParams {
   // 1/tau and 1 - omega/2 computed once on the device (the same IEEE float division as in the reference's
   // kernels, hoisted out of the per-cell work): fluid omega, thermal omega fluid/solid, source factor fluid/solid
   float omega_f, omega_tf, omega_ts, srcf_f, srcf_s;
+  unsigned* status;  // per-lattice device word: bit 0 = a bounded wait in a step kernel ran out
 };
 
 // One cell's view of a population array in global memory: the cell's own position (direction 0) and the same x
@@ -427,6 +428,103 @@ __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__
                   p.g);
 }
 
+// ---- thermal rows staged in shared memory (launch variant 1) ------------------------------------------
+// One block per row, blockDim = the row length. Thread 0 starts bulk copies (cp.async.bulk, completion counted on
+// an mbarrier) of the thermal input the row needs: the row's own 19 directions (one contiguous run) and, for the 16
+// directions whose source row differs (e_y or e_z != 0), that direction's run of the source row. The threads run
+// the fluid lattice from global memory meanwhile, then wait for the copies (bounded) and run the thermal lattice
+// from shared memory. Every cell runs the arithmetic of coupled_cell, so results are identical.
+template <typename S, int kT>
+struct StageQ {
+  static constexpr int kPad = 16 / (int)sizeof(S);  // 16 bytes of room on both sides of a run
+  static constexpr int kOwn = kPad + kQ * kT + kPad;
+  static constexpr int kSlot = kPad + kT + kPad;
+  static constexpr int kLen = kOwn + 16 * kSlot;  // elements
+};
+// a cell's view of the staged thermal input: own run (direction 0 at this x) and slot 0 (direction 3 at this x)
+template <typename S, int kT>
+struct SmemRows {
+  const S* c;
+  const S* s0;
+  __device__ __forceinline__ const S* own(int i) const { return c + i * kT; }
+  template <int I>
+  __device__ __forceinline__ const S* pull() const {
+    if (ey_of(I) == 0 && ez_of(I) == 0) return c + I * kT - ex_of(I);
+    return s0 + (I - 3) * StageQ<S, kT>::kSlot - ex_of(I);
+  }
+};
+
+__device__ __forceinline__ uint32_t sh_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ bool bar_wait_bounded(uint32_t bar, uint32_t parity) {
+  for (uint32_t i = 0; i < (1u << 22); ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+template <typename S, bool kMacro, bool kOwn, int kT>
+__global__ void __launch_bounds__(kT) coupled_qstage_kernel(const S* __restrict__ Pin, S* __restrict__ Pout,
+                                                            const S* __restrict__ Qin, S* __restrict__ Qout,
+                                                            const uint32_t* __restrict__ link,
+                                                            const float* __restrict__ qsrc,
+                                                            const float* __restrict__ u_in_ptr,
+                                                            float* __restrict__ rho_o, float* __restrict__ ux_o,
+                                                            float* __restrict__ uy_o, float* __restrict__ uz_o,
+                                                            const float* __restrict__ T0, StepParams p) {
+  using St = StageQ<S, kT>;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  S* sq = reinterpret_cast<S*>(sm_raw);
+  __shared__ __align__(8) uint64_t bar;
+  const uint32_t r = blockIdx.x, x = threadIdx.x;
+  const int lane = x & 31;
+  const uint32_t b = sh_addr(&bar);
+  if (x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(b), "r"(1u));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (x == 0) {
+    const uint32_t run = (uint32_t)(kT * sizeof(S));
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"((kQ + 16) * run) : "memory");
+    const S* row0 = Qin + p.g.guard;
+    bulk_copy(sh_addr(sq + St::kPad), row0 + (long long)r * kQ * kT, kQ * run, b);
+#pragma unroll
+    for (int i = 3; i < kQ; ++i) {
+      const long long rs = (long long)r - ey_of(i) - (long long)ez_of(i) * p.g.ny;  // guards cover rows off the grid
+      bulk_copy(sh_addr(sq + St::kOwn + (i - 3) * St::kSlot + St::kPad), row0 + (rs * kQ + i) * kT, run, b);
+    }
+  }
+  const bool valid = x < (uint32_t)p.g.nx;
+  const uint32_t c = r * (uint32_t)p.g.nx + x;
+  const uint32_t lw = valid ? __ldg(link + c) : ((uint32_t)kSolid << kTypeShift);
+  const unsigned fluid_lanes = __ballot_sync(0xffffffffu, valid && link_type(lw) != kSolid);
+  const uint32_t e0 = pop_base(r, x, p.g, kT);
+  float ux = 0.0f, uy = 0.0f, uz = 0.0f;
+  if (valid && link_type(lw) != kSolid)
+    fluid_cell<S, kMacro, 0, kT>(c, rows_at<kT>(Pin, e0, p.g, kT), Pout + e0, u_in_ptr, rho_o, ux_o, uy_o, uz_o, p,
+                                 lw, ux, uy, uz);
+  else if (valid)
+    solid_cell<S, kMacro, 0, kT>(c, rows_at<kT>(Pin, e0, p.g, kT), Pout + e0, rho_o, ux_o, uy_o, uz_o, p,
+                                 (fluid_lanes & sector_group<S>(lane)) != 0u);
+  const bool ok = bar_wait_bounded(b, 0);
+  if (!ok && x == 0) atomicOr(p.status, 1u);
+  if (valid && ok)
+    thermal_cell<S, kOwn, 2, kT>(c, SmemRows<S, kT>{sq + St::kPad + x, sq + St::kOwn + St::kPad + x}, Qout + e0,
+                                 qsrc, T0, p, lw, ux, uy, uz);
+  pad_fill<S, kT>(valid, fluid_lanes, __ballot_sync(0xffffffffu, valid), lane, Pout, Qout, e0, p.g);
+}
+
 // Arguments of one fused step launch; launch_coupled_step<S> (step_kernels.cuh, one translation unit per storage
 // type) picks the instantiation whose compile-time row length matches the lattice.
 struct StepLaunch {
@@ -441,6 +539,7 @@ struct StepLaunch {
   const float* T0;
   StepParams p;
   int block;
+  int variant;  // 0: one thread per row position; 1: thermal rows staged in shared memory (compile-time pitch)
   bool macro, own;
   cudaStream_t stream;
 };

@@ -10,6 +10,25 @@ namespace xac {
 template <typename S, bool kMacro, bool kOwn>
 void launch_step_rows(const StepLaunch& a) {
   const unsigned grid = (unsigned)(((long long)a.p.g.rows * a.p.g.pitch + a.block - 1) / a.block);
+  if (a.variant == 1 && a.p.g.pitch >= 64 && a.p.g.pitch <= 256) {
+    // one block per row; the kernel's compile-time row length is its block size
+#define XAC_QSTAGE(KT)                                                                                             \
+  coupled_qstage_kernel<S, kMacro, kOwn, KT><<<(unsigned)a.p.g.rows, KT, StageQ<S, KT>::kLen * sizeof(S),        \
+                                               a.stream>>>(                                                       \
+      (const S*)a.Pin, (S*)a.Pout, (const S*)a.Qin, (S*)a.Qout, a.link, a.qsrc, a.u_in, a.rho, a.ux, a.uy, a.uz, \
+      a.T0, a.p)
+    switch (a.p.g.pitch) {
+      case 64: XAC_QSTAGE(64); return;
+      case 96: XAC_QSTAGE(96); return;
+      case 128: XAC_QSTAGE(128); return;
+      case 160: XAC_QSTAGE(160); return;
+      case 192: XAC_QSTAGE(192); return;
+      case 224: XAC_QSTAGE(224); return;
+      case 256: XAC_QSTAGE(256); return;
+      default: break;
+    }
+#undef XAC_QSTAGE
+  }
 #define XAC_STEP(KT)                                                                                               \
   coupled_step_kernel<S, kMacro, kOwn, KT><<<grid, a.block, 0, a.stream>>>(                                     \
       (const S*)a.Pin, (S*)a.Pout, (const S*)a.Qin, (S*)a.Qout, a.link, a.qsrc, a.u_in, a.rho, a.ux, a.uy, a.uz, \
