@@ -231,8 +231,7 @@ def run_reference_arm(args):
 
 
 # ------------------------------------------------------------------------------------------------ GPU
-STEP_KERNELS = {0: "coupled_step_kernel<float>", 1: "coupled_step_grouped_kernel<float>",
-                2: "coupled_pair_kernel<float>"}
+STEP_KERNELS = {0: "coupled_step_kernel<float>", 1: "coupled_qstage_kernel<float>"}
 
 
 def warm_start_probe(n_designs=16, tol=TOL):

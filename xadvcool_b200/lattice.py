@@ -102,8 +102,8 @@ class Lattice:
         return int(v.value)
 
     def tune(self, block: int, variant: int):
-        """Launch shape of the fused step: threads per block and visiting order (0 memory order, 1 grouped by
-        cell class). Results are unaffected."""
+        """Launch shape of the fused step: threads per block (64, 128, 256) and variant (0: one thread per row
+        position; 1: one block per row with the thermal input staged in shared memory). Results are unaffected."""
         _capi.call("xac_lattice_tune", self._h, int(block), int(variant))
 
     def get_tune(self):
