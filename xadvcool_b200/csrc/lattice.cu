@@ -220,6 +220,7 @@ struct LatticeImpl {
     p.srcf_f = relax[3];
     p.srcf_s = relax[4];
     p.status = status;
+    p.reverse = (uint32_t)cur;  // sweep direction alternates with the buffer parity
     return p;
   }
 

@@ -113,6 +113,9 @@ struct StepParams {
   // 1/tau and 1 - omega/2 computed once on the device (the same IEEE float division as in the reference's
   // kernels, hoisted out of the per-cell work): fluid omega, thermal omega fluid/solid, source factor fluid/solid
   float omega_f, omega_tf, omega_ts, srcf_f, srcf_s;
+  // 1 = the step runs its blocks in reverse order. The host sets it on every other step, so each step starts on
+  // the rows the previous step wrote last, which are still in L2 (31.6 vs 32.4 us per 148x128x32 step)
+  uint32_t reverse;
   unsigned* status;  // per-lattice device word: bit 0 = a bounded wait in a step kernel ran out
 };
 
@@ -413,7 +416,8 @@ __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__
                                                            float* __restrict__ uy_o, float* __restrict__ uz_o,
                                                            const float* __restrict__ T0, StepParams p) {
   const int RL = row_len<kT>(p.g);
-  const uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t blk = p.reverse ? gridDim.x - 1u - blockIdx.x : blockIdx.x;
+  const uint32_t pos = blk * blockDim.x + threadIdx.x;
   const uint32_t r = pos / (uint32_t)RL, x = pos - r * (uint32_t)RL;
   if (r >= (uint32_t)p.g.rows) return;  // whole warps
   const int lane = threadIdx.x & 31;
@@ -486,7 +490,7 @@ __global__ void __launch_bounds__(kT) coupled_qstage_kernel(const S* __restrict_
   extern __shared__ __align__(16) unsigned char sm_raw[];
   S* sq = reinterpret_cast<S*>(sm_raw);
   __shared__ __align__(8) uint64_t bar;
-  const uint32_t r = blockIdx.x, x = threadIdx.x;
+  const uint32_t r = p.reverse ? gridDim.x - 1u - blockIdx.x : blockIdx.x, x = threadIdx.x;
   const int lane = x & 31;
   const uint32_t b = sh_addr(&bar);
   if (x == 0) {
