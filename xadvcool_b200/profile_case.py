@@ -3,6 +3,11 @@
     python -m xadvcool_b200.profile_case --save state.bin            # 4000 steps, then save the state
     python -m xadvcool_b200.profile_case --load state.bin --steps 2  # restore, then 2 steps in a profiler range
 
+    python -m xadvcool_b200.profile_case --warm 1 --steps 1 --chunk 100  # one step, then one 100-step call
+
+The third form runs the step loop as the solver does (100 steps per call, one CUDA graph), for captures of the
+DRAM traffic per launch with L2 as the previous step left it.
+
 The second form launches only a handful of small kernels before the profiled range
 (cudaProfilerStart/Stop), so a profiler attached with --profile-from-start off sees a developed-flow step
 after few prior launches.
@@ -51,6 +56,7 @@ def main(argv=None):
     ap.add_argument("--load")
     ap.add_argument("--warm", type=int, default=4000)
     ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--chunk", type=int, default=1, help="steps per call inside the profiled range")
     ap.add_argument("--precision", default="fp32")
     ap.add_argument("--block", type=int, default=128)
     ap.add_argument("--variant", type=int, default=0)
@@ -73,7 +79,7 @@ def main(argv=None):
     torch.cuda.synchronize()
     torch.cuda.profiler.start()
     for _ in range(a.steps):
-        lat.step(1)
+        lat.step(a.chunk)
     torch.cuda.synchronize()
     torch.cuda.profiler.stop()
     st = lat.stats()
