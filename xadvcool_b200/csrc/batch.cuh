@@ -87,6 +87,16 @@ __device__ __forceinline__ int find_slot(const uint32_t* prefix, int n, uint32_t
   }
   return lo;
 }
+// the same search over a copy of the prefix in shared memory, starting from slot lo (prefix[lo] <= t)
+__device__ __forceinline__ int find_slot_shared(const uint32_t* prefix, int lo, int n, uint32_t t) {
+  int hi = n;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (prefix[mid] <= t) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
 
 // tile = blockDim consecutive row positions (rows of `pitch` positions, x >= nx padding), one per thread
 template <typename S, bool kMacro, bool kOwn>
@@ -119,7 +129,7 @@ struct BatchRun {
 
 template <typename S>
 #ifndef XAC_BATCH_MIN_BLOCKS
-#define XAC_BATCH_MIN_BLOCKS 3
+#define XAC_BATCH_MIN_BLOCKS 4  // at most 64 registers; 3 and 5 blocks per SM measured slower
 #endif
 __global__ void __launch_bounds__(256, XAC_BATCH_MIN_BLOCKS) batch_persistent_kernel(BatchDesign* __restrict__ D, BatchCtl* __restrict__ ctl,
                                                                double* __restrict__ rows, BatchRun run) {
@@ -128,6 +138,7 @@ __global__ void __launch_bounds__(256, XAC_BATCH_MIN_BLOCKS) batch_persistent_ke
 #pragma unroll
   for (int k = 0; k < kNStats; ++k) spec.op[k] = (k == XAC_ST_MAX_V || k == XAC_ST_MAX_T) ? kMax : kSum;
   __shared__ BatchDesign dsh;
+  __shared__ uint32_t s_prefix[kMaxBatch + 1];
   long long step = ctl->step;
   for (int it = 0; it < run.steps; ++it) {
     if (*(volatile int*)&ctl->all_done || *(volatile int*)&ctl->err) break;
@@ -140,16 +151,23 @@ __global__ void __launch_bounds__(256, XAC_BATCH_MIN_BLOCKS) batch_persistent_ke
     const bool macro = stats || s1 == run.max_steps;
     const int cur = (int)(step & 1);
     // ---- one coupled step of every active design
+    // The tile prefix of the active designs goes to shared memory once per step. A block's tiles t rise, so
+    // their design slot k only moves forward: the search starts from the last slot, and the design's
+    // descriptor is copied to shared memory only when the slot changes.
+    for (int i = threadIdx.x; i <= na; i += blockDim.x) s_prefix[i] = __ldcg(ctl->prefix + i);
+    __syncthreads();
+    int kcur = -1;
     for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
-      const int k = find_slot(ctl->prefix, na, t);
-      const uint32_t tile = t - __ldcg(ctl->prefix + k);
-      {
-        // the design's descriptor, once per tile, into shared memory
+      const int k = (kcur >= 0 && t < s_prefix[kcur + 1]) ? kcur : find_slot_shared(s_prefix, kcur < 0 ? 0 : kcur, na, t);
+      if (k != kcur) {
+        __syncthreads();  // the previous design's tiles are done with dsh
         const uint32_t* src = reinterpret_cast<const uint32_t*>(&D[__ldcg(ctl->active + k)]);
         uint32_t* dst = reinterpret_cast<uint32_t*>(&dsh);
         for (uint32_t w = threadIdx.x; w < sizeof(BatchDesign) / 4; w += blockDim.x) dst[w] = __ldcg(src + w);
+        __syncthreads();
+        kcur = k;
       }
-      __syncthreads();
+      const uint32_t tile = t - s_prefix[k];
       const BatchDesign& d = dsh;
       if (own) {
         if (macro) batch_step_tile<S, true, true>(d, tile, cur);
@@ -159,7 +177,6 @@ __global__ void __launch_bounds__(256, XAC_BATCH_MIN_BLOCKS) batch_persistent_ke
       } else {
         batch_step_tile<S, false, false>(d, tile, cur);
       }
-      __syncthreads();
     }
     if (!grid_sync(ctl, run.spin_limit)) break;
     if (stats) {
