@@ -379,6 +379,9 @@ def run_gpu_arm(args):
                 "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                              "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                              "traffic": (round(tpc * cells) if tpc else None),
+                             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch inside "
+                                               "the 100-step loop (L2 as the previous step left it), "
+                                               "profiles/coupled_step_gyroid148.md",
                              "kernel": STEP_KERNELS[shape["variant"]],
                              "alg_bytes_per_launch": alg_bytes, "mean_launch_us": round(step_ms * 1e3, 3)},
                 "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": h2d,
