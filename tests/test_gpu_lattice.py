@@ -58,7 +58,7 @@ def test_config1_straight_fin_plate_2000_steps_bit_exact(cuda):
     assert float(np.abs(u).max()) < 0.17
 
 
-@pytest.mark.parametrize("chunks", [[1], [2], [1, 1, 1], [7], [8], [3, 20, 1], [50]])
+@pytest.mark.parametrize("chunks", [[1], [2], [1, 1, 1], [7], [8], [3, 20, 1], [50], [1200], [5, 1031]])
 def test_random_channel_step_chunking_bit_exact(chunks, cuda):
     mask, hs = channel(11)
     kw = dict(tau_fluid=0.57, heat_power=3e-3, u_inlet_val=0.04, Pr=3.0, k_ratio=30.0)

@@ -273,6 +273,33 @@ struct LatticeImpl {
     return XAC_OK;
   }
 
+  // n >= 8 plain steps from the cached graph of n steps for the current buffer parity (captured on first use)
+  int launch_graph(cudaStream_t s, int n) {
+    auto key = std::make_pair(n, cur);
+    auto it = graphs.find(key);
+    if (it == graphs.end()) {
+      if (!capture) XAC_CUDA(cudaStreamCreateWithFlags(&capture, cudaStreamNonBlocking));
+      const int saved = cur;
+      cudaGraph_t graph = nullptr;
+      XAC_CUDA(cudaStreamBeginCapture(capture, cudaStreamCaptureModeThreadLocal));
+      launch_plain(capture, n);
+      cudaError_t e = cudaStreamEndCapture(capture, &graph);
+      cur = saved;
+      if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
+      cudaGraphExec_t exec = nullptr;
+      e = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
+      it = graphs.emplace(key, exec).first;
+    }
+    XAC_CUDA(cudaGraphLaunch(it->second, s));
+    if (n & 1) cur ^= 1;
+    return XAC_OK;
+  }
+
+  // Long runs go as graphs of at most kGraphSteps steps (an even count, so the same graph serves every chunk);
+  // each chunk's last step also writes rho/u, which changes no population.
+  static constexpr int kGraphSteps = 512;
   int steps(int n, cudaStream_t s) {
     if (n <= 0) return XAC_OK;
     if (own_pending) {
@@ -283,30 +310,18 @@ struct LatticeImpl {
       XAC_CUDA(cudaGetLastError());
     }
     if (n > 0) {
+      const int total = n;
+      for (; n > kGraphSteps; n -= kGraphSteps) {
+        int r = launch_graph(s, kGraphSteps);
+        if (r != XAC_OK) return r;
+      }
       if (n >= 8) {
-        auto key = std::make_pair(n, cur);
-        auto it = graphs.find(key);
-        if (it == graphs.end()) {
-          if (!capture) XAC_CUDA(cudaStreamCreateWithFlags(&capture, cudaStreamNonBlocking));
-          const int saved = cur;
-          cudaGraph_t graph = nullptr;
-          XAC_CUDA(cudaStreamBeginCapture(capture, cudaStreamCaptureModeThreadLocal));
-          launch_plain(capture, n);
-          cudaError_t e = cudaStreamEndCapture(capture, &graph);
-          cur = saved;
-          if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
-          cudaGraphExec_t exec = nullptr;
-          e = cudaGraphInstantiate(&exec, graph, 0);
-          cudaGraphDestroy(graph);
-          if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
-          it = graphs.emplace(key, exec).first;
-        }
-        XAC_CUDA(cudaGraphLaunch(it->second, s));
-        if (n & 1) cur ^= 1;
+        int r = launch_graph(s, n);
+        if (r != XAC_OK) return r;
       } else {
         launch_plain(s, n);
       }
-      step += n;
+      step += total;
       XAC_CUDA(cudaGetLastError());
     }
     macro_step = step;
