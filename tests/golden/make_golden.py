@@ -9,6 +9,11 @@ does not, so the outputs are committed).
                   HDF5 group is served from memory) on the seeded cases of oracle.validate_ref.validation_case.
 * parquet_rows.json — stratified rows of dataset/metadata.parquet (inputs and golden scalars of the
                   reference's GPU runs), excluding gaussian_hotspots rows whose seed is process-salted.
+* failed_rows.json — stratified entries of dataset/failed_samples.json (designs the reference rejected as
+                  invalid geometry, diverged or unphysical) with their parameters, recovered by regenerating the
+                  reference's sample list (generate_samples, 200 per design, seed 42: the dataset's 10,000 ids,
+                  every failed id among them) and hashing each parameter set into its sample id as
+                  generate_dataset.py:368-369 does. Solved designs exclude gaussian_hotspots heat maps.
 
 Usage: python tests/golden/make_golden.py [/path/to/reference]
 """
@@ -131,6 +136,38 @@ def _validate_reference(ref: Path):
     return run
 
 
+def sample_id(params: dict) -> str:
+    """generate_dataset.py:366-369."""
+    ps = json.dumps(params, sort_keys=True) + "|coolant=water"
+    return f"{params['design_name'].replace(' ', '_')}_water_{hashlib.md5(ps.encode()).hexdigest()[:8]}"
+
+
+def write_failed_rows(ref: Path, gd):
+    failed = json.loads((ref / "dataset" / "failed_samples.json").read_text())
+    found = {}
+    for name in gd.DESIGN_CONFIGS:
+        for params in gd.generate_samples(name, 200, seed=42):
+            found[sample_id(params)] = params
+    missing = [k for k in failed if k not in found]
+    assert not missing, f"{len(missing)} failed ids not in the regenerated sample list"
+    by = {}
+    for sid, reason in sorted(failed.items()):
+        p = found[sid]
+        cat = reason.split(" (")[0]
+        if cat != "invalid geometry" and p["heat_source_type"] == "gaussian_hotspots":
+            continue  # heat map seeded by the process-salted hash(sample_id)
+        by.setdefault((p["design_name"], cat), []).append((sid, reason, p))
+    quota = {"invalid geometry": 6, "diverged": 2, "unphysical": 2}
+    rng = np.random.default_rng(4321)
+    out = []
+    for (name, cat), lst in sorted(by.items()):
+        for i in sorted(rng.choice(len(lst), size=min(quota[cat], len(lst)), replace=False).tolist()):
+            sid, reason, p = lst[i]
+            out.append({"sample_id": sid, "category": cat, "reason": reason, "params": p})
+    (HERE / "failed_rows.json").write_text(json.dumps(out, indent=1, sort_keys=True))
+    return len(out)
+
+
 def main(ref: Path):
     import pandas as pd
     geometry, gd = _import_reference(ref)
@@ -207,7 +244,9 @@ def main(ref: Path):
         vcases.append({"seed": seed, "checks": {k: (bool(v) if isinstance(v, (bool, np.bool_)) else float(v))
                                                 for k, v in res.items() if k != "sample_id"}})
     (HERE / "validate.json").write_text(json.dumps(vcases, indent=1))
-    print(f"wrote {len(out_rows)} rows, {len(designs)} masks, {len(heat)} heat maps, {len(mcases)} metric cases")
+    n_failed = write_failed_rows(ref, gd)
+    print(f"wrote {len(out_rows)} rows, {len(designs)} masks, {len(heat)} heat maps, {len(mcases)} metric cases, "
+          f"{n_failed} failed-sample rows")
 
 
 if __name__ == "__main__":

@@ -9,6 +9,10 @@ as Parquet with the reference's columns.
     w = DatasetWriter("out/")
     w.add_lattice("sample_0001", lat, design, result, elapsed_s)   # after lat.run(...)
     w.close()                                                       # -> out/metadata.parquet
+
+The reference's admission rules decide which solves become samples: ``is_valid_geometry`` before the solve
+(generate_dataset.py:281-292), then ``divergence_reason`` and ``plausibility_reason`` after it (:438-483). Their
+reason strings are the ones the reference records in failed_samples.json.
 """
 from __future__ import annotations
 
@@ -27,6 +31,56 @@ METADATA_COLUMNS = [
 ]
 METRIC_KEYS = ["R_th", "Nu", "f_friction", "P_pump", "COP", "Q_vol", "T_max_surface", "T_avg_surface",
                "delta_T_max", "sigma_T", "fluid_temp_rise"]
+
+# generate_dataset.py:278-279
+MIN_POROSITY = 0.15
+MAX_POROSITY = 0.90
+BC_SOLID = 1
+
+
+def is_valid_geometry(mask, buf: int = 10):
+    """generate_dataset.py:281-292: porosity of the core (x outside the inlet/outlet buffers) within
+    [MIN_POROSITY, MAX_POROSITY], and neither the first nor the last core x plane fully solid. Returns
+    (valid, porosity); a rejected design is recorded as ``f"invalid geometry (porosity={porosity:.2%})"``."""
+    m = np.asarray(mask)
+    core = m[buf:-buf, :, :]
+    porosity = float(1.0 - np.sum(core == BC_SOLID) / core.size)
+    if porosity < MIN_POROSITY or porosity > MAX_POROSITY:
+        return False, porosity
+    inlet = m[buf, 1:-1, 4:-2]
+    outlet = m[-(buf + 1), 1:-1, 4:-2]
+    if np.all(inlet == BC_SOLID) or np.all(outlet == BC_SOLID):
+        return False, porosity
+    return True, porosity
+
+
+def divergence_reason(u, T):
+    """generate_dataset.py:438-447 on the solved fields (reference layout: u (nx,ny,nz,3), T (nx,ny,nz), host
+    float32): the reason string, or None when the solve did not diverge."""
+    max_v = np.max(np.linalg.norm(np.asarray(u), axis=-1))
+    max_T = np.max(np.asarray(T))
+    Ma = max_v * (3.0 ** 0.5)
+    if np.isnan(max_v) or Ma > 0.3 or np.isnan(max_T) or max_T > 1e4:
+        return f"diverged (max_v={max_v:.2e}, Ma={Ma:.2f}, max_T={max_T:.2e})"
+    return None
+
+
+def plausibility_reason(metrics: dict, converged: bool):
+    """generate_dataset.py:458-483 on compute_macroscopic_metrics' output and the solve's converged flag: the
+    reason string, or None when the sample is kept."""
+    Nu, R_th, COP, rise = metrics["Nu"], metrics["R_th"], metrics["COP"], metrics["fluid_temp_rise"]
+    reasons = []
+    if Nu < 0 or Nu > 2000 or np.isnan(Nu):
+        reasons.append(f"Nu={Nu:.1f}")
+    if R_th < 0 or R_th > 1000 or np.isnan(R_th):
+        reasons.append(f"R_th={R_th:.1f}")
+    if COP < 0 or np.isnan(COP):
+        reasons.append(f"COP={COP:.2e}")
+    if rise < 0 or np.isnan(rise):
+        reasons.append(f"fluid_temp_rise={rise:.2e}")
+    if not converged:
+        reasons.append("not converged")
+    return f"unphysical ({', '.join(reasons)})" if reasons else None
 
 
 def metadata_row(sample_id, design: dict, mask_shape, scalars: dict, steps: int, converged: bool, elapsed_s: float,
