@@ -292,11 +292,22 @@ def screen(seeds, steps=500):
     return [s for s, r in zip(seeds, res) if not r["diverged"]], [s for s, r in zip(seeds, res) if r["diverged"]]
 
 
-def compare_batched(model, seeds, *, max_steps=150000, tol=1e-6, warm_min_steps=1000):
+def _vs(a, ref, ok_a, ok_ref):
+    """Relative delta_P / R_th differences of batch ``a`` against batch ``ref`` over designs converged in both."""
+    both = [j for j in range(len(ok_a)) if ok_a[j] and ok_ref[j]]
+    dp = [_rel(a["scalars"][j]["delta_P"], ref["scalars"][j]["delta_P"]) for j in both]
+    rt = [_rel(a["scalars"][j]["R_th"], ref["scalars"][j]["R_th"]) for j in both]
+    return {"compared": len(both), "dP_rel_max": max(dp) if dp else None, "Rth_rel_max": max(rt) if rt else None,
+            "Rth_rel_median": float(np.median(rt)) if rt else None,
+            "within_half_percent": sum(1 for x, y in zip(dp, rt) if x <= 5e-3 and y <= 5e-3)}
+
+
+def compare_batched(model, seeds, *, max_steps=150000, tol=1e-6, warm_min_steps=1000, tight_tol=None):
     """Batched solves of the held-out designs whose cold start passes the divergence guard, cold and warm (same
     designs, same residual): wall seconds per converged design from mask upload to scalars, steps, and the
     scalar agreement per design. The designs whose cold start trips the guard are then solved warm, to count
-    those the warm start solves."""
+    those the warm start solves. With ``tight_tol`` the same designs are also solved cold to that residual, and
+    both the cold and the warm scalars are compared with those of the tight solve (``vs_tight``)."""
     good, bad = screen(seeds)
     out = {"screened_out": len(bad)}
     dg = [design(s) for s in good]
@@ -311,6 +322,10 @@ def compare_batched(model, seeds, *, max_steps=150000, tol=1e-6, warm_min_steps=
                within_half_percent=sum(1 for a, b in zip(dp, rt) if a <= 5e-3 and b <= 5e-3),
                step_ratio=sum(c["steps"]) / max(sum(w["steps"]), 1),
                speedup=c["s_per_converged_design"] / w["s_per_converged_design"])
+    if tight_tol is not None:
+        t = _batched(dg, None, max_steps=max_steps, tol=tight_tol, warm_min_steps=warm_min_steps)
+        out["vs_tight"] = {"tol": tight_tol, "tight_converged": t["converged"],
+                           "cold": _vs(c, t, c["ok"], t["ok"]), "warm": _vs(w, t, w["ok"], t["ok"])}
     if bad:
         r = _batched([design(s) for s in bad], model, max_steps=max_steps, tol=tol, warm_min_steps=warm_min_steps)
         out["warm_cold_tripped"] = {k: r[k] for k in ("designs", "converged", "diverged", "steps", "wall_s")}
