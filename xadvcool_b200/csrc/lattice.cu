@@ -162,6 +162,61 @@ int reduction_blocks(long long n) {
 
 }  // namespace
 
+// ---------------------------------------------------------------- device-resident run loop
+// State of xac_lattice_run's convergence loop while a CUDA graph runs it: one while-node iteration is
+// stats_every steps, T, the stats, and run_decision_kernel, which repeats the host loop's arithmetic
+// (simulation.py:121-156) in double and sets the graph's loop condition.
+struct RunCtl {
+  long long start;      // lattice step count when the run began
+  long long step;       // steps of this run done
+  long long min_steps;  // no convergence before this many steps of the run
+  long long max_iters;  // stats intervals this launch may run
+  long long iters;
+  int stats_every, constant_power, stop, diverged;
+  double tol_ke, tol_T, target_power;
+  double prev_ke, prev_max_T, prev_Q, d_ke, dT, dQ;
+  float u_in;
+  int pad;
+  double last[kNStats];
+};
+
+static __global__ void run_decision_kernel(const double* __restrict__ st, RunCtl* c, float* u_in_dev,
+                                           cudaGraphConditionalHandle h) {
+  c->step += c->stats_every;
+  c->iters += 1;
+  const double max_v = st[XAC_ST_MAX_V], ke = st[XAC_ST_SUM_KE], max_T = st[XAC_ST_MAX_T], Q_out = st[XAC_ST_Q_OUT];
+  const long long at = c->start + c->step;
+  const bool past = at > c->stats_every;
+  c->d_ke = past ? fabs(ke - c->prev_ke) / (c->prev_ke + 1e-9) / c->stats_every : 0.0;
+  c->dT = past ? fabs(max_T - c->prev_max_T) / (c->prev_max_T + 1e-9) / c->stats_every : 0.0;
+  c->dQ = past ? fabs(Q_out - c->prev_Q) / (fabs(c->prev_Q) + 1e-12) / c->stats_every : 1.0;
+  c->prev_ke = ke;
+  c->prev_max_T = max_T;
+  c->prev_Q = Q_out;
+  if (c->constant_power && at > 2000) {
+    double ue = (double)c->u_in;
+    const double rin = st[XAC_ST_C_IN] > 0 ? st[XAC_ST_SUM_RHO_IN] / st[XAC_ST_C_IN] : 1.0;
+    const double rout = st[XAC_ST_C_OUT] > 0 ? st[XAC_ST_SUM_RHO_OUT] / st[XAC_ST_C_OUT] : 1.0;
+    const double dP = (rin - rout) / 3.0;
+    const double pw = dP * (ue * st[XAC_ST_C_IN]);
+    ue = ue + 0.005 * (c->target_power - pw);
+    ue = ue < 0.0001 ? 0.0001 : (ue > 0.15 ? 0.15 : ue);
+    c->u_in = (float)ue;
+    *u_in_dev = (float)ue;
+  }
+  for (int k = 0; k < kNStats; ++k) c->last[k] = st[k];
+  bool stop = false;
+  if (c->step > c->min_steps && c->d_ke < c->tol_ke && c->dT < c->tol_T && c->dQ < c->tol_T) {
+    stop = true;
+  } else if (st[XAC_ST_NONFINITE] > 0 || max_v > 0.17 || max_T > 1e4) {
+    c->diverged = 1;
+    stop = true;
+  }
+  if (c->iters >= c->max_iters) stop = true;
+  c->stop = stop ? 1 : 0;
+  cudaGraphSetConditional(h, stop ? 0u : 1u);
+}
+
 // ---------------------------------------------------------------- the lattice object
 struct LatticeImpl {
   Geom g{};
@@ -203,6 +258,9 @@ struct LatticeImpl {
   long long T_step = 0;       // T array holds the field of this step
   cudaStream_t capture = nullptr;
   std::map<std::pair<int, int>, cudaGraphExec_t> graphs;  // (n, parity) -> n steps with macro output at the end
+  std::map<std::pair<int, int>, cudaGraphExec_t> run_graphs;  // (stats_every, parity) -> device-resident run loop
+  RunCtl* run_ctl = nullptr;       // device
+  RunCtl* run_ctl_host = nullptr;  // pinned
   std::mutex mu;
 
   StepParams params() const {
@@ -226,6 +284,9 @@ struct LatticeImpl {
 
   ~LatticeImpl() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    for (auto& kv : run_graphs) cudaGraphExecDestroy(kv.second);
+    cudaFree(run_ctl);
+    if (run_ctl_host) cudaFreeHost(run_ctl_host);
     for (void* b : {P[0], P[1], Qb[0], Qb[1]}) cudaFree(b);
     cudaFree(type);
     cudaFree(link);
@@ -325,6 +386,71 @@ struct LatticeImpl {
       XAC_CUDA(cudaGetLastError());
     }
     macro_step = step;
+    return XAC_OK;
+  }
+
+  // The device-resident run loop for the current buffer parity: a graph whose while node repeats
+  // { every plain steps, T, stats, run_decision_kernel } until the decision kernel clears the condition.
+  // every must be even (the parity is the same at each iteration).
+  int run_graph(int every, cudaGraphExec_t* out) {
+    auto key = std::make_pair(every, cur);
+    auto it = run_graphs.find(key);
+    if (it != run_graphs.end()) {
+      *out = it->second;
+      return XAC_OK;
+    }
+    if (!capture) XAC_CUDA(cudaStreamCreateWithFlags(&capture, cudaStreamNonBlocking));
+    if (!run_ctl) {
+      XAC_CUDA(cudaMalloc(&run_ctl, sizeof(RunCtl)));
+      XAC_CUDA(cudaMallocHost(&run_ctl_host, sizeof(RunCtl)));
+    }
+    cudaGraph_t graph = nullptr;
+    XAC_CUDA(cudaGraphCreate(&graph, 0));
+    cudaGraphConditionalHandle h;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h, graph, 1u, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&node, graph, nullptr, 0, &np);
+    const int saved = cur;
+    if (e == cudaSuccess)
+      e = cudaStreamBeginCaptureToGraph(capture, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(graph);
+      return cuda_status(e, "run loop graph");
+    }
+    launch_plain(capture, every);
+    const StepParams p = params();
+    const unsigned grid = grid_for(g.ncell, kBlock);
+    switch (precision) {
+      case XAC_FP16:
+        thermal_finalize_kernel<__half><<<grid, kBlock, 0, capture>>>((const __half*)Qb[cur], link, T, p);
+        break;
+      case XAC_BF16:
+        thermal_finalize_kernel<__nv_bfloat16><<<grid, kBlock, 0, capture>>>((const __nv_bfloat16*)Qb[cur], link,
+                                                                             T, p);
+        break;
+      default:
+        thermal_finalize_kernel<float><<<grid, kBlock, 0, capture>>>((const float*)Qb[cur], link, T, p);
+    }
+    const auto spec = stats_spec();
+    const int ntiles = (int)stats_tiles(g.ncell);
+    stats_partials_kernel<<<ntiles, kStatsTile, 0, capture>>>(view(), spec, rows);
+    combine_rows_kernel<kNStats><<<1, 32 * kNStats, 0, capture>>>(rows, ntiles, spec, red_out);
+    run_decision_kernel<<<1, 1, 0, capture>>>(red_out, run_ctl, u_in, h);
+    cudaGraph_t body = nullptr;
+    e = cudaStreamEndCapture(capture, &body);
+    cur = saved;
+    cudaGraphExec_t exec = nullptr;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_status(e, "run loop graph");
+    run_graphs.emplace(key, exec);
+    *out = exec;
     return XAC_OK;
   }
 
@@ -708,6 +834,8 @@ int xac_lattice_tune(xac_lattice* lat, int block, int variant) {
   if (L.tune_block != block || L.tune_variant != variant) {
     for (auto& kv : L.graphs) cudaGraphExecDestroy(kv.second);
     L.graphs.clear();
+    for (auto& kv : L.run_graphs) cudaGraphExecDestroy(kv.second);
+    L.run_graphs.clear();
   }
   L.tune_block = block;
   L.tune_variant = variant;
@@ -845,6 +973,7 @@ int xac_lattice_run(xac_lattice* lat, const xac_run_opts* o, xac_run_result* res
   const long long start = L.step;
   long long step = 0;
   int diverged = 0;
+  bool tried_device = false;
   while (step < o->max_steps) {
     int chunk = o->stats_every - (int)((start + step) % o->stats_every);
     if (step + chunk > o->max_steps) chunk = (int)(o->max_steps - step);
@@ -879,6 +1008,65 @@ int xac_lattice_run(xac_lattice* lat, const xac_run_opts* o, xac_run_result* res
     if (st[XAC_ST_NONFINITE] > 0 || max_v > 0.17 || max_T > 1e4) {
       diverged = 1;
       break;
+    }
+    // After the first check, the remaining whole stats intervals run as one graph launch with the loop on the
+    // device (same arithmetic, same decisions); the host reads the loop state back once.
+    const long long iters = (o->max_steps - step) / o->stats_every;
+    if (!tried_device && o->stats_every % 2 == 0 && o->stats_every >= 8 && iters >= 2 && !L.own_pending &&
+        (start + step) % o->stats_every == 0) {
+      tried_device = true;
+      cudaStream_t s = as_stream(stream);
+      std::lock_guard<std::mutex> g(L.mu);
+      cudaGraphExec_t ex = nullptr;
+      r = L.run_graph(o->stats_every, &ex);
+      if (r != XAC_OK) return r;
+      RunCtl& c = *L.run_ctl_host;
+      std::memset(&c, 0, sizeof(c));
+      c.start = start;
+      c.step = step;
+      c.min_steps = min_steps;
+      c.max_iters = iters;
+      c.stats_every = o->stats_every;
+      c.constant_power = o->constant_power;
+      c.tol_ke = o->tol_ke;
+      c.tol_T = o->tol_T;
+      c.target_power = o->target_power;
+      c.prev_ke = prev_ke;
+      c.prev_max_T = prev_max_T;
+      c.prev_Q = prev_Q;
+      c.d_ke = d_ke;
+      c.dT = dT;
+      c.dQ = dQ;
+      c.u_in = L.u_in_host;
+      XAC_CUDA(cudaMemcpyAsync(L.run_ctl, &c, sizeof(RunCtl), cudaMemcpyHostToDevice, s));
+      XAC_CUDA(cudaGraphLaunch(ex, s));
+      XAC_CUDA(cudaMemcpyAsync(&c, L.run_ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, s));
+      XAC_CUDA(cudaStreamSynchronize(s));
+      L.step += c.step - step;
+      L.macro_step = L.step;
+      L.T_step = L.step;
+      L.u_in_host = c.u_in;
+      step = c.step;
+      prev_ke = c.prev_ke;
+      prev_max_T = c.prev_max_T;
+      prev_Q = c.prev_Q;
+      d_ke = c.d_ke;
+      dT = c.dT;
+      dQ = c.dQ;
+      std::memcpy(res->last_stats, c.last, sizeof(c.last));
+      if (L.tune_variant == 1) {  // the staged kernel's bounded wait reports here
+        unsigned stw = 0;
+        XAC_CUDA(cudaMemcpy(&stw, L.status, sizeof(stw), cudaMemcpyDeviceToHost));
+        if (stw) {
+          set_error("xac_lattice_run: a staged step kernel gave up waiting for its copies (status %u)", stw);
+          return XAC_ETIMEOUT;
+        }
+      }
+      if (c.diverged) {
+        diverged = 1;
+        break;
+      }
+      if (step > min_steps && d_ke < o->tol_ke && dT < o->tol_T && dQ < o->tol_T) break;
     }
   }
   res->steps = step;
