@@ -274,6 +274,11 @@ typedef struct xac_run_result {
     double last_stats[XAC_NSTATS];
 } xac_run_result;
 
+/* src/simulation.py:102-162: steps, stats every stats_every steps, the relative-rate convergence test, the
+ * divergence guard and the constant-power pump. After the first check the remaining whole intervals run as one
+ * CUDA graph launch whose conditional while node repeats {stats_every steps, T, stats, decision kernel} (even
+ * stats_every >= 8); the decision kernel does the host loop's double arithmetic, so results do not depend on
+ * where the loop runs. Blocks until the run ends. */
 int xac_lattice_run(xac_lattice *lat, const xac_run_opts *opts, xac_run_result *res, void *stream);
 
 /* ========================================================================== *
