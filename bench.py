@@ -387,7 +387,7 @@ def run_gpu_arm(args):
                              "kernel": STEP_KERNELS[shape["variant"]],
                              "alg_bytes_per_launch": alg_bytes, "mean_launch_us": round(step_ms * 1e3, 3)},
                 "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": h2d,
-                        "d2h_bytes_per_step": d2h, "s_per_converged_design": round(e2e_max, 4),
+                        "d2h_bytes_per_step": d2h, "s_per_solve": round(e2e_max, 4),
                         "solver_steps": res["steps"], "converged": res["converged"]},
                 "gpu_launches": args.steps * (STEPS_PER_BENCH_STEP + 3),
                 "launch_shape": {"block": shape["block"], "variant": shape["variant"], "autotuned": shape["table"]},
