@@ -359,8 +359,10 @@ def run_gpu_arm(args):
     e2e_max = max_over_ranks(e2e_s, world)
     e2e_lups = sum_over_ranks(cells * res["steps"], world)
     e2e_value = e2e_lups / e2e_max / 1e6
-    h2d = mask.size * 4 + hs.size * 4
-    d2h = cells * 5 * 4 + (res["steps"] // STEPS_PER_BENCH_STEP) * 17 * 8
+    # int32 mask + float32 heat source in; rho, u, T out; the stats of the first check (17 doubles) and the run
+    # loop's control block (272 bytes, written before and read after the device-resident loop)
+    h2d = mask.size * 4 + hs.size * 4 + 272
+    d2h = cells * 5 * 4 + 17 * 8 + 272
 
     # side measurements of the other forms, after the headline numbers (they load the GPU heavily)
     forms = forms_probe(dev, mask, lat_kw, shape) if rank == 0 else None
