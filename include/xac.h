@@ -306,11 +306,14 @@ int xac_conv3d_status(int *flags);
  * mixed_design) evaluated per cell. No reference counterpart on the device: the reference builds masks with numpy
  * (src/geometry.py:339-526). The host draws the random parameters and fills the spec.
  * ========================================================================== */
+#define XAC_DESIGN_EMPTY 0      /* no solid inside the frame (src/geometry.py:381-383) */
 #define XAC_DESIGN_STRAIGHT 1   /* p0 = channel width, p1 = channel count (src/geometry.py:385-434) */
 #define XAC_DESIGN_PIN_FIN 2    /* p0 = pin radius, p1 = pitch: two interleaved square lattices of pins */
 #define XAC_DESIGN_GYROID 3     /* p0 = cell size L, p1 = threshold t: solid where the TPMS value > t */
 #define XAC_DESIGN_SCHWARZ_P 4
 #define XAC_DESIGN_SCHWARZ_D 5
+#define XAC_DESIGN_BELOW 16     /* with a TPMS family: solid where the value < p1, as generate_mask does
+                                   (src/geometry.py:497-503) */
 #define XAC_DESIGN_MAX_HOT 8
 typedef struct xac_design_spec {
     int nx, ny, nz;       /* lattice, reference layout [nx][ny][nz] */

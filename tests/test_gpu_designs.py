@@ -35,3 +35,41 @@ def test_rejects_bad_spec(cuda):
     spec["hot"] = spec["hot"][:9] if len(spec["hot"]) >= 9 else spec["hot"] + [(1.0, 1.0, 4.0, 0.5)] * 9
     with pytest.raises(Exception):
         G.build(spec)
+
+
+# ---- the reference's generate_mask families (src/geometry.py:339-526) on the device
+import hashlib  # noqa: E402
+import json  # noqa: E402
+from pathlib import Path  # noqa: E402
+
+GOLD = json.loads((Path(__file__).resolve().parent / "golden" / "designs.json").read_text())
+ROWS = json.loads((Path(__file__).resolve().parent / "golden" / "parquet_rows.json").read_text())
+
+
+def _sha(t):
+    return hashlib.sha256(np.ascontiguousarray(t.cpu().numpy().astype(np.int32)).tobytes()).hexdigest()
+
+
+def test_reference_families_match_the_reference_masks(cuda):
+    """All 72 golden states (6 design types x 4 feature sizes x 3 spacings), hashed from the reference's own
+    generate_mask: the device mask has the same bytes."""
+    bad = [m["state"] for m in GOLD["masks"] if _sha(G.reference_design(m["state"])[0]) != m["sha256"]]
+    assert not bad, bad
+
+
+def test_dataset_rows_build_on_the_device(cuda):
+    """The 45 dataset rows' masks (hashed from the reference) and their floor heat maps."""
+    for r in ROWS:
+        state = {"design_type": r["design_idx"], "feature_size": r["feature_size"], "spacing": r["spacing"],
+                 "buffer_size": 10}
+        mask, heat = G.reference_design(state, r["heat_source_type"])
+        assert _sha(mask) == r["mask_sha256"], r["sample_id"]
+        host = H.floor_heat_source(tuple(mask.shape), H.HEAT_SOURCE_REGISTRY[r["heat_source_type"]](128, 128))
+        assert np.array_equal(heat.cpu().numpy(), host)
+
+
+def test_reference_design_rejects_bad_family(cuda):
+    spec = H.reference_spec({"design_type": 1, "feature_size": 3.0, "spacing": 3.0, "buffer_size": 10})
+    spec["below"] = True  # only TPMS families take the below-threshold convention
+    with pytest.raises(Exception):
+        G.build(spec)

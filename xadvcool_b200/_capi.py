@@ -73,7 +73,8 @@ class DesignSpec(C.Structure):
     ]
 
 
-DESIGN_FAMILIES = {"straight": 1, "pin_fin": 2, "gyroid": 3, "schwarz_p": 4, "schwarz_d": 5}
+DESIGN_FAMILIES = {"empty": 0, "straight": 1, "pin_fin": 2, "gyroid": 3, "schwarz_p": 4, "schwarz_d": 5}
+DESIGN_BELOW = 16  # TPMS: solid where the value is below the threshold (generate_mask's convention)
 
 
 class RunResult(C.Structure):

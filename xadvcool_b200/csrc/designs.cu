@@ -1,4 +1,6 @@
-// Seeded cold-plate designs built on the device: the per-cell evaluation of xadvcool_b200.designs.build_from_spec
+// Cold-plate designs built on the device: the reference's generate_mask families (src/geometry.py:339-526,
+// parameters mapped on the host by xadvcool_b200.designs.reference_spec) and the seeded benchmark designs, the
+// per-cell evaluation of xadvcool_b200.designs.build_from_spec
 // (straight channels, src/geometry.py:385-434; staggered pin fins; gyroid / Schwarz P / Schwarz D TPMS,
 // src/geometry.py:476-495; the frame of src/geometry.py:510-524) and the Gaussian-hotspot floor map. The random
 // draws stay on the host (numpy's generator), so a seed gives the same design either way. Every expression keeps
@@ -49,10 +51,11 @@ __global__ void design_kernel(xac_design_spec sp, int32_t* __restrict__ mask, fl
   const int core = nx - 2 * sp.buf;
   bool solid = false;
   const int xc = x - sp.buf;
-  if (xc >= 0 && xc < core) {
-    if (sp.family == XAC_DESIGN_STRAIGHT) {
+  const int family = sp.family & ~XAC_DESIGN_BELOW;
+  if (xc >= 0 && xc < core && family != XAC_DESIGN_EMPTY) {
+    if (family == XAC_DESIGN_STRAIGHT) {
       solid = straight_wall(y, ny, (int)sp.p0, (int)sp.p1);
-    } else if (sp.family == XAC_DESIGN_PIN_FIN) {
+    } else if (family == XAC_DESIGN_PIN_FIN) {
       const double radius = sp.p0, pitch = sp.p1, h = pitch / 2;
       const long long ip = (long long)pitch;
       const double ax = (double)(xc % ip) - h, ay = (double)(y % ip) - h;
@@ -64,15 +67,16 @@ __global__ void design_kernel(xac_design_spec sp, int32_t* __restrict__ mask, fl
       const double omega = 2.0 * M_PI / sp.p0;
       const double wx = (double)xc * omega, wy = (double)y * omega, wz = (double)z * omega;
       double f;
-      if (sp.family == XAC_DESIGN_GYROID) {
+      if (family == XAC_DESIGN_GYROID) {
         f = (sin(wx) * cos(wy) + sin(wy) * cos(wz)) + sin(wz) * cos(wx);
-      } else if (sp.family == XAC_DESIGN_SCHWARZ_P) {
+      } else if (family == XAC_DESIGN_SCHWARZ_P) {
         f = (cos(wx) + cos(wy)) + cos(wz);
       } else {
         f = ((sin(wx) * sin(wy) * sin(wz) + sin(wx) * cos(wy) * cos(wz)) + cos(wx) * sin(wy) * cos(wz)) +
             cos(wx) * cos(wy) * sin(wz);
       }
-      solid = f > sp.p1 && !(xc < sp.margin || xc >= core - sp.margin);
+      const bool inside = (sp.family & XAC_DESIGN_BELOW) ? f < sp.p1 : f > sp.p1;
+      solid = inside && !(xc < sp.margin || xc >= core - sp.margin);
     }
   }
   int m = solid ? XAC_BC_SOLID : XAC_BC_FLUID;
@@ -103,12 +107,14 @@ extern "C" int xac_design_build(const xac_design_spec* spec, int32_t* mask_dev, 
   const xac_design_spec& s = *spec;
   XAC_REQUIRE(s.nx >= 3 && s.ny >= 3 && s.nz > kBase + kTop && s.buf >= 0 && 2 * s.buf < s.nx,
               "xac_design_build: bad shape %d x %d x %d (buffer %d)", s.nx, s.ny, s.nz, s.buf);
-  XAC_REQUIRE(s.family >= XAC_DESIGN_STRAIGHT && s.family <= XAC_DESIGN_SCHWARZ_D, "xac_design_build: family %d",
-              s.family);
+  const int fam = s.family & ~XAC_DESIGN_BELOW;
+  XAC_REQUIRE(fam >= XAC_DESIGN_EMPTY && fam <= XAC_DESIGN_SCHWARZ_D &&
+                  (!(s.family & XAC_DESIGN_BELOW) || fam >= XAC_DESIGN_GYROID),
+              "xac_design_build: family %d", s.family);
   XAC_REQUIRE(s.n_hot >= 0 && s.n_hot <= XAC_DESIGN_MAX_HOT, "xac_design_build: %d hotspots (at most %d)", s.n_hot,
               XAC_DESIGN_MAX_HOT);
-  XAC_REQUIRE(s.family != XAC_DESIGN_PIN_FIN || s.p1 >= 1.0, "xac_design_build: pin pitch must be >= 1");
-  XAC_REQUIRE(s.family < XAC_DESIGN_GYROID || s.p0 > 0.0, "xac_design_build: TPMS cell size must be positive");
+  XAC_REQUIRE(fam != XAC_DESIGN_PIN_FIN || s.p1 >= 1.0, "xac_design_build: pin pitch must be >= 1");
+  XAC_REQUIRE(fam < XAC_DESIGN_GYROID || s.p0 > 0.0, "xac_design_build: TPMS cell size must be positive");
   const long long n = (long long)s.nx * s.ny * s.nz;
   design_kernel<<<(unsigned)((n + 255) / 256), 256, 0, as_stream(stream)>>>(s, mask_dev, heat_dev);
   XAC_CUDA(cudaGetLastError());

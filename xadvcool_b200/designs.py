@@ -76,26 +76,51 @@ def tpms_field(kind: int, shape, cell_size: float) -> np.ndarray:
     raise ValueError(f"unknown TPMS kind {kind}")
 
 
-def generate_mask(state: dict) -> np.ndarray:
-    """src/geometry.py:339-526 with ``state`` keys design_type, feature_size, spacing, buffer_size."""
-    nx, ny, nz = CORE_NX, CORE_NY, CORE_NZ
-    design = int(state["design_type"])
-    design = min(max(design, 0), len(DESIGN_NAMES) - 1)
+def _generate_params(state: dict):
+    """src/geometry.py:339-379: (design, buffer, channel width, channel count, pin diameter, pin pitch, TPMS
+    threshold C, TPMS cell size) from a GUI/sampler state."""
+    design = min(max(int(state["design_type"]), 0), len(DESIGN_NAMES) - 1)
     buf = int(state["buffer_size"])
-    mask = np.full((nx + 2 * buf, ny, nz), BC_FLUID, dtype=np.int32)
-    solid = np.zeros((nx, ny, nz), dtype=bool)
     raw_width = state.get("feature_size", 3.0)
     raw_count = state.get("spacing", 3.0)
     width = max(2, int(raw_width * 2.0))
     target = max(4, int(raw_count * 4.0))
-    n_channels = max(2, min(target, int((ny - 1) / (width + 1))))
+    n_channels = max(2, min(target, int((CORE_NY - 1) / (width + 1))))
+    d_pin = max(2, int(raw_width * 2.0))
+    pitch = max(d_pin + 2, int(raw_count * 3.0))
+    C = 0.8 - ((raw_width - 1.0) / 9.0) * 1.6
+    cell_size = 20.0 + ((raw_count - 1.0) / 9.0) * 80.0
+    return design, buf, width, n_channels, d_pin, pitch, C, cell_size
+
+
+def reference_spec(state: dict) -> dict:
+    """generate_mask's design as the parameters of the device evaluation (xadvcool_b200.device_designs):
+    family, lattice shape, buffer, and the family's two numbers (channel width / count, pin radius / pitch, TPMS
+    cell size / threshold with solid below it and 5 fluid x cells at each end of the core)."""
+    design, buf, width, n_channels, d_pin, pitch, C, cell_size = _generate_params(state)
+    spec = {"shape": (CORE_NX + 2 * buf, CORE_NY, CORE_NZ), "buf": buf, "hot": [], "background": 0.0}
+    if design == 0:
+        spec.update(family="empty", p=(0.0, 0.0))
+    elif design == 1:
+        spec.update(family="straight", p=(float(width), float(n_channels)))
+    elif design == 2:
+        spec.update(family="pin_fin", p=(d_pin / 2.0, float(pitch)))
+    else:
+        spec.update(family=["gyroid", "schwarz_p", "schwarz_d"][design - 3], p=(cell_size, C), below=True, margin=5)
+    return spec
+
+
+def generate_mask(state: dict) -> np.ndarray:
+    """src/geometry.py:339-526 with ``state`` keys design_type, feature_size, spacing, buffer_size."""
+    nx, ny, nz = CORE_NX, CORE_NY, CORE_NZ
+    design, buf, width, n_channels, _, _, C, cell_size = _generate_params(state)
+    mask = np.full((nx + 2 * buf, ny, nz), BC_FLUID, dtype=np.int32)
+    solid = np.zeros((nx, ny, nz), dtype=bool)
     if design == 1:
         _straight_channels(solid, width, n_channels)
     elif design == 2:
-        _pin_fins(solid, raw_width, raw_count)
+        _pin_fins(solid, state.get("feature_size", 3.0), state.get("spacing", 3.0))
     elif design in (3, 4, 5):
-        C = 0.8 - ((raw_width - 1.0) / 9.0) * 1.6
-        cell_size = 20.0 + ((raw_count - 1.0) / 9.0) * 80.0
         solid[:, :, :] = tpms_field(design, (nx, ny, nz), cell_size) < C
         solid[:5] = False
         solid[-5:] = False
