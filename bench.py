@@ -276,7 +276,9 @@ def forms_probe(dev, mask, lat_kw, shape):
         m, h, u, _ = designs.mixed_design(s)
         ds.append(dict(mask=m, heat_source=h, tau_fluid=0.56, u_inlet_val=u))
     cells = sum(d["mask"].size for d in ds)
+    tiles = autotune.autotune_batch(ds, device=dev)  # scratch batches; cached per design set
     b = Batch(ds, device=dev)
+    autotune.apply_batch(b, ds)
     torch.cuda.synchronize(dev)
     t = time.perf_counter()
     b.run(max_steps=1000, stats_every=100, tol_ke=0.0, tol_T=0.0)
@@ -285,6 +287,7 @@ def forms_probe(dev, mask, lat_kw, shape):
     b.close()
     out["batch64_mixed_mlups"] = round(cells * 1000 / dt / 1e6, 1)
     out["batch64_cells"] = cells
+    out["batch64_tile"] = {"block": tiles["block"], "autotuned_us_per_step": tiles["table"]}
     out["warm_start"] = warm_start_probe()
     return out
 

@@ -99,3 +99,26 @@ def test_batch_constant_power_equals_solo(spl, cuda):
         for x, y in zip([t.cpu().numpy() for t in lat.fields()], f_solo):
             assert np.array_equal(x, y)
     b.close()
+
+
+def test_batch_tile_autotune(cuda, tmp_path, monkeypatch):
+    """The batch autotuner times every tile on scratch batches, caches the winner, and sets it; the tuned batch
+    still solves exactly as the solo lattices do."""
+    from xadvcool_b200 import autotune
+    monkeypatch.setenv("XAC_AUTOTUNE_CACHE", str(tmp_path / "cache.json"))
+    ds = small_designs()
+    res = autotune.autotune_batch(ds, steps=200)
+    assert res["block"] in autotune.BATCH_BLOCKS
+    assert sorted(res["table"]) == sorted(str(b) for b in autotune.BATCH_BLOCKS)
+    assert autotune.autotune_batch(ds, steps=200) == res  # cached
+    b = Batch(ds)
+    autotune.apply_batch(b, ds, steps=200)
+    assert b.get_tune()[0] == res["block"]
+    run = dict(max_steps=600, stats_every=100, tol_ke=0.0, tol_T=0.0)
+    out = b.run(**run)
+    for i, d in enumerate(ds):
+        ref, f_ref = solo(d, **run)
+        assert out[i]["steps"] == ref["steps"] and out[i]["d_ke"] == ref["d_ke"]
+        for a, c in zip((t.cpu().numpy() for t in b.lattice(i).fields()), f_ref):
+            assert np.array_equal(a, c)
+    b.close()

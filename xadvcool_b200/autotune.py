@@ -1,4 +1,5 @@
-"""Autotuner for the launch shape of the fused coupled step (threads per block x visiting order).
+"""Autotuners for the launch shape of the fused coupled step (threads per block x visiting order) and for the
+tile of the persistent batched kernel.
 
 The shape changes only the schedule, never a result (every cell runs the same arithmetic). Candidates are
 timed with CUDA events on a scratch lattice built from the same inputs, so the caller's lattice does not
@@ -87,6 +88,60 @@ def autotune(mask, *, heat_source=None, precision="fp32", device="cuda", steps=1
     if use_cache:
         cache[key] = res
         _store_cache(cache)
+    return res
+
+
+BATCH_BLOCKS = (64, 128, 256)
+
+
+def _time_batch(designs, precision, dev, block, steps, stream) -> float:
+    """Microseconds per step of a fresh batch of ``designs`` run ``steps`` steps with tile ``block`` (a batch
+    runs once, from step 0)."""
+    from .batch import Batch
+    b = Batch(designs, precision=precision, device=dev)
+    try:
+        _, spl = b.get_tune()
+        b.tune(block, spl)
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        b.run(max_steps=steps, stats_every=100, tol_ke=0.0, tol_T=0.0)
+        t1.record(stream)
+        t1.synchronize()
+        return round(t0.elapsed_time(t1) * 1e3 / steps, 3)
+    finally:
+        b.close()
+
+
+def autotune_batch(designs, *, precision="fp32", device="cuda", steps=300, use_cache=True) -> dict:
+    """Fastest tile of the persistent batched kernel (threads per block = row positions per tile) for this set of
+    designs: each candidate runs ``steps`` steps (stats every 100, no retirement) on a scratch batch built from
+    the same designs, timed with CUDA events from the launch to the end of the run; the caller's batch does not
+    advance. Cached per (device, number of designs, total cells, precision, solid fraction). Returns {"block",
+    "us_per_step", "table"}."""
+    dev = torch.device(device)
+    cells = sum(int(np.asarray(d["mask"]).size) for d in designs)
+    solid = sum(int((np.asarray(d["mask"]) == 1).sum()) for d in designs) / max(cells, 1)
+    name = torch.cuda.get_device_name(dev).replace(" ", "_")
+    key = f"batch|{name}|{len(designs)}|{cells}|{precision}|solid{round(solid, 2):.2f}"
+    cache = _load_cache() if use_cache else {}
+    if key in cache:
+        return cache[key]
+    stream = torch.cuda.current_stream(dev)
+    _time_batch(designs, precision, dev, BATCH_BLOCKS[-1], steps, stream)  # warm-up (module load, first launch)
+    table = {str(b): _time_batch(designs, precision, dev, b, steps, stream) for b in BATCH_BLOCKS}
+    best = min(table, key=table.get)
+    res = {"block": int(best), "us_per_step": table[best], "table": table}
+    if use_cache:
+        cache[key] = res
+        _store_cache(cache)
+    return res
+
+
+def apply_batch(batch, designs, **kw) -> dict:
+    """Autotune the tile for ``designs`` and set it on ``batch`` (built from the same designs)."""
+    res = autotune_batch(designs, device=batch.device, **kw)
+    _, spl = batch.get_tune()
+    batch.tune(res["block"], spl)
     return res
 
 
