@@ -58,6 +58,11 @@ CASES = {
     "every50": dict(max_steps=1500, every=50, tol=1e-5, min_steps=200, pump=False, u=0.01),
     # the divergence guard trips on the device (at step 200, the first check after the host's)
     "diverges": dict(max_steps=3000, every=100, tol=1e-5, min_steps=0, pump=False, u=0.04),
+    # 16-bit population storage
+    "fp16": dict(max_steps=3000, every=100, tol=1e-3, min_steps=500, pump=False, u=0.01, precision="fp16"),
+    "bf16": dict(max_steps=2000, every=100, tol=1e-12, min_steps=0, pump=False, u=0.01, precision="bf16"),
+    # a warm start (fields from a short solve): the first step reads them unstreamed, then the device loop
+    "warm": dict(max_steps=3000, every=100, tol=1e-3, min_steps=300, pump=False, u=0.01, warm=True),
 }
 
 
@@ -65,12 +70,22 @@ CASES = {
 def test_device_loop_matches_the_host_loop(case, cuda):
     c = CASES[case]
     mask, hs, _, _ = designs.gyroid_design(7, nx=60, ny=32, nz=16)
-    kw = dict(heat_source=hs, tau_fluid=0.56, u_inlet_val=c["u"], heat_power=0.05)
+    kw = dict(heat_source=hs, tau_fluid=0.56, u_inlet_val=c["u"], heat_power=0.05,
+              precision=c.get("precision", "fp32"))
+    init = None
+    if c.get("warm"):
+        with Lattice(mask, **kw) as w:
+            w.step(400)
+            init = [t.clone() for t in w.fields()]
     a = Lattice(mask, **kw)
+    if init:
+        a.init_fields(*init)
     got = a.run(max_steps=c["max_steps"], stats_every=c["every"], tol_ke=c["tol"], tol_T=c["tol"],
                 min_steps=c["min_steps"], pump_mode="constant_power" if c["pump"] else "constant_flow",
                 target_power=0.002)
     b = Lattice(mask, **kw)
+    if init:
+        b.init_fields(*init)
     want = host_run(b, c["max_steps"], c["every"], c["tol"], c["tol"], c["min_steps"], constant_power=c["pump"],
                     target_power=0.002)
     for k in ("steps", "converged", "diverged", "d_ke", "dT_conv", "dQ_conv", "u_inlet_final"):
