@@ -351,7 +351,10 @@ def run_gpu_arm(args):
     tpc = ncu_traffic_per_cell()
     lat.close()
 
-    # e2e: a full solve through the public API, host numpy in and out
+    # e2e: a full solve through the public API, host numpy in and out; one short untimed solve first warms the
+    # path (kernel modules of the stats and run-loop code, host staging buffers of the field read-back)
+    run_simulation(mask, max_steps=2 * STEPS_PER_BENCH_STEP + 1, tau_fluid=TAU, heat_power=POWER, u_inlet_val=u_in,
+                   heat_source=hs, tol_ke=TOL, tol_T=TOL, Pr=PR, k_ratio=K_RATIO, silent=True, device=str(dev))
     barrier(world)
     torch.cuda.synchronize(dev)
     t = time.perf_counter()
