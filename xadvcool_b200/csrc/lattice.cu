@@ -400,10 +400,8 @@ struct LatticeImpl {
       return XAC_OK;
     }
     if (!capture) XAC_CUDA(cudaStreamCreateWithFlags(&capture, cudaStreamNonBlocking));
-    if (!run_ctl) {
-      XAC_CUDA(cudaMalloc(&run_ctl, sizeof(RunCtl)));
-      XAC_CUDA(cudaMallocHost(&run_ctl_host, sizeof(RunCtl)));
-    }
+    if (!run_ctl) XAC_CUDA(cudaMalloc(&run_ctl, sizeof(RunCtl)));
+    if (!run_ctl_host) XAC_CUDA(cudaMallocHost(&run_ctl_host, sizeof(RunCtl)));
     cudaGraph_t graph = nullptr;
     XAC_CUDA(cudaGraphCreate(&graph, 0));
     cudaGraphConditionalHandle h;
