@@ -123,7 +123,7 @@ int xac_stats_fields(const float *rho, const float *u, const float *T, const int
                      double *out_host, void *stream);
 /* No counterpart in the reference. The same stats as xac_stats_fields for callers that cannot allocate device or
  * pinned memory (code running inside a stream capture, or under a memory budget owned by another allocator):
- * it calls no allocator. Its scratch is a fixed 1.1 MB array in the library's device image, held by every GPU
+ * it calls no allocator. Its scratch is a fixed 278 KB array in the library's device image, held by every GPU
  * that loads the library; lattices above 2,097,152 cells are rejected (XAC_EINVAL). The result (XAC_NSTATS
  * doubles) goes to the caller's DEVICE buffer out_dev, asynchronously on `stream`. All calls on a device share
  * the scratch, so calls whose GPU work overlaps race. The first call on a device looks up the scratch address;

@@ -3,7 +3,7 @@
 // Every resident block loops over steps. In a step it takes tiles (one cell per thread, `blockDim` cells per
 // tile) from the concatenated tile list of the still-active designs, then meets the other blocks at a grid
 // barrier. On a stats step (every stats_every steps, src/simulation.py:123) the blocks also finalise T and
-// reduce the stats of every active design into 256-cell tile rows, one block per design combines its rows and
+// reduce the stats of every active design into 1024-cell tile rows, one block per design combines its rows and
 // applies the relative-rate convergence test and divergence guard of src/simulation.py:134-156, and converged
 // or diverged designs retire: the next steps skip their tiles and the remaining work is redistributed over all
 // blocks. The per-tile reduction is the single-lattice one, so a design solved in a batch takes exactly the
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(256, XAC_BATCH_MIN_BLOCKS) batch_persistent_ke
     }
     if (!grid_sync(ctl, run.spin_limit)) break;
     if (stats) {
-      // ---- T of the new state and 256-cell tile rows of stats
+      // ---- T of the new state and 1024-cell tile rows of stats
       const uint32_t stotal = __ldcg(ctl->stat_prefix + na);
       for (uint32_t t = blockIdx.x; t < stotal; t += gridDim.x) {
         const int k = find_slot(ctl->stat_prefix, na, t);

@@ -437,7 +437,7 @@ struct LatticeImpl {
     }
     const auto spec = stats_spec();
     const int ntiles = (int)stats_tiles(g.ncell);
-    stats_partials_kernel<<<ntiles, kStatsTile, 0, capture>>>(view(), spec, rows);
+    stats_partials_kernel<<<ntiles, kStatsBlock, 0, capture>>>(view(), spec, rows);
     combine_rows_kernel<kNStats><<<1, 32 * kNStats, 0, capture>>>(rows, ntiles, spec, red_out);
     run_decision_kernel<<<1, 1, 0, capture>>>(red_out, run_ctl, u_in, h);
     cudaGraph_t body = nullptr;
@@ -496,7 +496,7 @@ struct LatticeImpl {
 int run_stats(const FieldView& v, double* rows, double* dev_out, double* host_out, cudaStream_t s) {
   const auto spec = stats_spec();
   const int ntiles = (int)stats_tiles((long long)v.nx * v.ny * v.nz);
-  stats_partials_kernel<<<ntiles, kStatsTile, 0, s>>>(v, spec, rows);
+  stats_partials_kernel<<<ntiles, kStatsBlock, 0, s>>>(v, spec, rows);
   combine_rows_kernel<kNStats><<<1, 32 * kNStats, 0, s>>>(rows, ntiles, spec, dev_out);
   XAC_CUDA(cudaGetLastError());
   XAC_CUDA(cudaMemcpyAsync(host_out, dev_out, kNStats * sizeof(double), cudaMemcpyDeviceToHost, s));

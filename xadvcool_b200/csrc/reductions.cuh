@@ -140,24 +140,30 @@ __device__ __forceinline__ void stats_accumulate(const FieldView& v, int x, int 
   acc[XAC_ST_COUNT_T] += 1.0;
 }
 
-// One row of partial stats for the 256-cell tile `tile` (cells enumerated x fastest). The tile is reduced as 8
-// chunks of 32 cells, each by one warp with a fixed butterfly, and the chunks are combined in order by one
-// thread: the row does not depend on the block size that computes it. Every thread of the block must call.
-constexpr int kStatsTile = 256;
+// One row of partial stats for the 1024-cell tile `tile` (cells enumerated x fastest). The tile is reduced as 8
+// chunks of 128 cells, each by one warp: every lane adds its 4 cells (lane, lane+32, lane+64, lane+96 of the
+// chunk) in order, then a fixed butterfly combines the lanes; the chunks are combined in order by one thread.
+// The row does not depend on the block size that computes it. Every thread of the block must call.
+constexpr int kStatsTile = 1024;   // cells per partial row
+constexpr int kStatsChunk = 128;   // cells per warp chunk
+constexpr int kStatsBlock = 256;   // threads of the kernels that compute the rows
 __device__ __forceinline__ void stats_tile_row(const FieldView& v, long long tile, const ReduceSpec<kNStats>& spec,
                                                double* __restrict__ row) {
-  __shared__ double chunk[kStatsTile / 32][kNStats];
+  __shared__ double chunk[kStatsTile / kStatsChunk][kNStats];
   const long long n = (long long)v.nx * v.ny * v.nz;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  for (int ch = warp; ch < kStatsTile / 32; ch += nwarps) {
+  for (int ch = warp; ch < kStatsTile / kStatsChunk; ch += nwarps) {
     double acc[kNStats];
 #pragma unroll
     for (int k = 0; k < kNStats; ++k) acc[k] = identity(spec.op[k]);
-    const long long i = tile * kStatsTile + ch * 32 + lane;
-    if (i < n) {  // lattices stay below 2^31 cells: 32-bit decomposition
-      const unsigned iu = (unsigned)i, nx = (unsigned)v.nx, ny = (unsigned)v.ny;
-      const unsigned t = iu / nx;
-      stats_accumulate(v, (int)(iu - t * nx), (int)(t % ny), (int)(t / ny), acc);
+#pragma unroll
+    for (int j = 0; j < kStatsChunk / 32; ++j) {
+      const long long i = tile * kStatsTile + ch * kStatsChunk + j * 32 + lane;
+      if (i < n) {  // lattices stay below 2^31 cells: 32-bit decomposition
+        const unsigned iu = (unsigned)i, nx = (unsigned)v.nx, ny = (unsigned)v.ny;
+        const unsigned t = iu / nx;
+        stats_accumulate(v, (int)(iu - t * nx), (int)(t % ny), (int)(t / ny), acc);
+      }
     }
 #pragma unroll
     for (int k = 0; k < kNStats; ++k) {
@@ -171,7 +177,7 @@ __device__ __forceinline__ void stats_tile_row(const FieldView& v, long long til
   if (threadIdx.x < kNStats) {
     const int k = threadIdx.x;
     double a = identity(spec.op[k]);
-    for (int ch = 0; ch < kStatsTile / 32; ++ch) a = combine(spec.op[k], a, chunk[ch][k]);
+    for (int ch = 0; ch < kStatsTile / kStatsChunk; ++ch) a = combine(spec.op[k], a, chunk[ch][k]);
     row[k] = a;
   }
   __syncthreads();

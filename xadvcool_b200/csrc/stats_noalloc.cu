@@ -9,7 +9,7 @@
 //
 // Limits and rules, also stated in include/xac.h:
 //   * at most kNoAllocMaxCells = 2,097,152 cells per call; larger lattices are rejected with XAC_EINVAL;
-//   * the scratch (8,192 x 17 doubles, 1.1 MB) lives in every GPU that loads the library, until exit;
+//   * the scratch (2,048 x 17 doubles, 278 KB) lives in every GPU that loads the library, until exit;
 //   * every call on a device shares that one array: calls whose GPU work overlaps (other streams, other host
 //     threads) race on it; each call rewrites all the partial rows it reads, so nothing needs clearing;
 //   * the first call on each device resolves the array's device address (cudaGetSymbolAddress, with that device
@@ -26,7 +26,7 @@ constexpr long long kNoAllocMaxCells = 1LL << 21;
 constexpr int kNoAllocMaxTiles = (int)((kNoAllocMaxCells + kStatsTile - 1) / kStatsTile);
 constexpr int kMaxDevices = 64;
 
-// Partial rows of the stats reduction, one per 256-cell tile. In host code this name is only a handle for
+// Partial rows of the stats reduction, one per 1024-cell tile. In host code this name is only a handle for
 // cudaGetSymbolAddress: kernels receive the device address returned by it.
 static __device__ __align__(256) double g_noalloc_rows[kNoAllocMaxTiles * kNStats];
 
@@ -88,7 +88,7 @@ extern "C" int xac_stats_fields_noalloc(const float* rho, const float* u, const 
   const auto spec = stats_spec();
   const int ntiles = (int)stats_tiles(n);
   cudaStream_t s = as_stream(stream);
-  noalloc_rows_kernel<<<ntiles, kStatsTile, 0, s>>>(v, spec, rows);
+  noalloc_rows_kernel<<<ntiles, kStatsBlock, 0, s>>>(v, spec, rows);
   combine_rows_kernel<kNStats><<<1, 32 * kNStats, 0, s>>>(rows, ntiles, spec, out_dev);
   XAC_CUDA(cudaGetLastError());
   return XAC_OK;
