@@ -63,6 +63,8 @@ CASES = {
     "bf16": dict(max_steps=2000, every=100, tol=1e-12, min_steps=0, pump=False, u=0.01, precision="bf16"),
     # a warm start (fields from a short solve): the first step reads them unstreamed, then the device loop
     "warm": dict(max_steps=3000, every=100, tol=1e-3, min_steps=300, pump=False, u=0.01, warm=True),
+    # the lattice already advanced 37 steps: the first interval is 63 steps long
+    "offset": dict(max_steps=2000, every=100, tol=1e-12, min_steps=0, pump=False, u=0.01, pre=37),
 }
 
 
@@ -80,12 +82,14 @@ def test_device_loop_matches_the_host_loop(case, cuda):
     a = Lattice(mask, **kw)
     if init:
         a.init_fields(*init)
+    a.step(c.get("pre", 0))
     got = a.run(max_steps=c["max_steps"], stats_every=c["every"], tol_ke=c["tol"], tol_T=c["tol"],
                 min_steps=c["min_steps"], pump_mode="constant_power" if c["pump"] else "constant_flow",
                 target_power=0.002)
     b = Lattice(mask, **kw)
     if init:
         b.init_fields(*init)
+    b.step(c.get("pre", 0))
     want = host_run(b, c["max_steps"], c["every"], c["tol"], c["tol"], c["min_steps"], constant_power=c["pump"],
                     target_power=0.002)
     for k in ("steps", "converged", "diverged", "d_ke", "dT_conv", "dQ_conv", "u_inlet_final"):
