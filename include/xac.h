@@ -151,6 +151,11 @@ int xac_thermal_macroscopic(const float *g, float *T, int nx, int ny, int nz, vo
 /* Test-only operators of validate_analytical.py (kept off the product path). */
 /* validate_analytical.py:21-30 dirichlet_thermal_bc_kernel(g, T_val, x_plane, ny, nz) */
 int xac_test_dirichlet_plane(float *g, float T_val, int x_plane, int nx, int ny, int nz, void *stream);
+/* Test-only: makes the library's bounded waits run out on purpose (an mbarrier that nothing arrives on, as in
+ * the staged step kernel; the batched kernel's grid barrier with a block that never arrives), each after `limit`
+ * polls (1..2^20). status_out: bit 0 the mbarrier wait gave up, bit 1 the grid barrier gave up, bit 2 the grid
+ * barrier recorded XAC_ETIMEOUT; 7 when every wait reported. The context stays usable. */
+int xac_test_bounded_waits(unsigned limit, unsigned *status_out, void *stream);
 /* validate_analytical.py:255-273 periodic_streaming_kernel and :607-621 periodic_thermal_streaming_kernel */
 int xac_test_periodic_stream(const float *f_post, float *f_streamed, int nx, int ny, int nz, void *stream);
 /* validate_analytical.py:377-395 forced_bgk_collision_kernel(f_old, f_eq, f_new, mask, tau, force_x) */

@@ -1,0 +1,34 @@
+"""Failure detection without a GPU fault: the library's bounded waits (the staged step kernel's mbarrier wait,
+the batched kernel's grid barrier) are made to run out on purpose, through a test-only entry point, with a wait
+that nothing completes. Each must give up after its limit and report, and the context must stay usable."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from xadvcool_b200 import _capi, designs
+from xadvcool_b200._tensors import stream_ptr
+from xadvcool_b200.lattice import Lattice
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("limit", [1, 1000])
+def test_bounded_waits_give_up_and_report(limit, cuda):
+    st = C.c_uint(0)
+    _capi.call("xac_test_bounded_waits", limit, C.byref(st), stream_ptr(torch.device("cuda")))
+    assert st.value == 7  # mbarrier wait gave up, grid barrier gave up and recorded XAC_ETIMEOUT
+    # the context is still usable: a solve right after runs, on the staged kernel, with finite stats
+    mask = designs.straight_fin_plate()
+    with Lattice(mask, tau_fluid=0.6, heat_power=1e-4, u_inlet_val=0.05, Pr=2.0, k_ratio=100.0) as lat:
+        lat.tune(128, 1)  # the staged kernel, whose wait is the one exercised above
+        lat.step(20)
+        s = lat.stats()
+    assert np.isfinite(s).all() and s[16] == 0
+
+
+def test_bounded_waits_reject_bad_limit(cuda):
+    st = C.c_uint(0)
+    with pytest.raises(_capi.XacError):
+        _capi.call("xac_test_bounded_waits", 0, C.byref(st), None)

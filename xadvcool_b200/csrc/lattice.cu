@@ -959,6 +959,59 @@ int xac_lattice_load_state(xac_lattice* lat, const void* host_src, size_t bytes,
   return XAC_OK;
 }
 
+// ---- test-only: bounded waits that run out ----------------------------------------------------------------
+// The staged step kernel waits on an mbarrier, the batched kernel at a grid barrier; both waits are bounded.
+// Here one block waits on an mbarrier that nothing arrives on, and a two-block grid meets at the batch kernel's
+// grid barrier with one block that never arrives: both waits must give up after `limit` polls and report,
+// and the context stays usable.
+static __global__ void test_mbarrier_timeout_kernel(uint32_t limit, unsigned* status) {
+  __shared__ __align__(8) uint64_t bar;
+  const uint32_t b = sh_addr(&bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(b), "r"(1u));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const bool ok = bar_wait_bounded(b, 0, limit);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (!ok) atomicOr(status, 1u);
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(b) : "memory");
+  }
+}
+
+static __global__ void test_grid_barrier_timeout_kernel(BatchCtl* ctl, unsigned long long limit, unsigned* status) {
+  if (blockIdx.x == gridDim.x - 1) return;  // this block never arrives
+  if (!grid_sync(ctl, limit) && threadIdx.x == 0) atomicOr(status, 2u);
+}
+
+extern "C" int xac_test_bounded_waits(unsigned limit, unsigned* status_out, void* stream) {
+  XAC_REQUIRE(status_out, "xac_test_bounded_waits: null pointer");
+  XAC_REQUIRE(limit > 0 && limit <= (1u << 20), "xac_test_bounded_waits: limit %u out of (0, 2^20]", limit);
+  cudaStream_t s = as_stream(stream);
+  unsigned* st = nullptr;
+  BatchCtl* ctl = nullptr;
+  XAC_CUDA(cudaMalloc(&st, sizeof(unsigned)));
+  cudaError_t e = cudaMalloc(&ctl, sizeof(BatchCtl));
+  if (e == cudaSuccess) e = cudaMemsetAsync(st, 0, sizeof(unsigned), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ctl, 0, sizeof(BatchCtl), s);
+  if (e == cudaSuccess) {
+    test_mbarrier_timeout_kernel<<<1, 32, 0, s>>>(limit, st);
+    test_grid_barrier_timeout_kernel<<<2, 32, 0, s>>>(ctl, (unsigned long long)limit, st);
+    e = cudaGetLastError();
+  }
+  unsigned host = 0;
+  int err = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&host, st, sizeof(host), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&err, &ctl->err, sizeof(err), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(st);
+  cudaFree(ctl);
+  if (e != cudaSuccess) return cuda_status(e, "xac_test_bounded_waits");
+  *status_out = host | (err == XAC_ETIMEOUT ? 4u : 0u);  // bit 2: the grid barrier recorded XAC_ETIMEOUT
+  return XAC_OK;
+}
+
 // simulation.py:102-162
 int xac_lattice_run(xac_lattice* lat, const xac_run_opts* o, xac_run_result* res, void* stream) {
   XAC_REQUIRE(lat && o && res, "xac_lattice_run: null pointer");

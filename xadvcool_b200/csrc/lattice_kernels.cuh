@@ -464,8 +464,8 @@ __device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_
                "l"(src), "r"(bytes), "r"(bar)
                : "memory");
 }
-__device__ __forceinline__ bool bar_wait_bounded(uint32_t bar, uint32_t parity) {
-  for (uint32_t i = 0; i < (1u << 22); ++i) {
+__device__ __forceinline__ bool bar_wait_bounded(uint32_t bar, uint32_t parity, uint32_t limit = 1u << 22) {
+  for (uint32_t i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
