@@ -156,6 +156,9 @@ int xac_test_dirichlet_plane(float *g, float T_val, int x_plane, int nx, int ny,
  * polls (1..2^20). status_out: bit 0 the mbarrier wait gave up, bit 1 the grid barrier gave up, bit 2 the grid
  * barrier recorded XAC_ETIMEOUT; 7 when every wait reported. The context stays usable. */
 int xac_test_bounded_waits(unsigned limit, unsigned *status_out, void *stream);
+/* Test-only: the convolution kernels' mbarrier wait on a barrier nothing completes, limited to `limit` polls
+ * (1..2^20); it must set bit 0 of the flags xac_conv3d_status returns. */
+int xac_test_conv_wait_timeout(unsigned limit, void *stream);
 /* validate_analytical.py:255-273 periodic_streaming_kernel and :607-621 periodic_thermal_streaming_kernel */
 int xac_test_periodic_stream(const float *f_post, float *f_streamed, int nx, int ny, int nz, void *stream);
 /* validate_analytical.py:377-395 forced_bgk_collision_kernel(f_old, f_eq, f_new, mask, tau, force_x) */

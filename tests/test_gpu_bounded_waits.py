@@ -32,3 +32,11 @@ def test_bounded_waits_reject_bad_limit(cuda):
     st = C.c_uint(0)
     with pytest.raises(_capi.XacError):
         _capi.call("xac_test_bounded_waits", 0, C.byref(st), None)
+
+
+def test_conv_wait_gives_up_and_reports(cuda):
+    from xadvcool_b200 import surrogate as S
+    S.kernel_status()  # clears the flags
+    _capi.call("xac_test_conv_wait_timeout", 1000, stream_ptr(torch.device("cuda")))
+    assert S.kernel_status() & 1
+    assert S.kernel_status() == 0  # read-and-clear

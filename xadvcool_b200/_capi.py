@@ -103,6 +103,7 @@ SIGNATURES = {
     "xac_thermal_macroscopic": [_vp, _vp, _i, _i, _i, _vp],
     "xac_test_dirichlet_plane": [_vp, _f, _i, _i, _i, _i, _vp],
     "xac_test_bounded_waits": [C.c_uint, _vp, _vp],
+    "xac_test_conv_wait_timeout": [C.c_uint, _vp],
     "xac_test_periodic_stream": [_vp, _vp, _i, _i, _i, _vp],
     "xac_test_forced_bgk": [_vp, _vp, _vp, _vp, _f, _f, _i, _i, _i, _vp],
     "xac_test_periodic_stream_solids": [_vp, _vp, _vp, _i, _i, _i, _vp],

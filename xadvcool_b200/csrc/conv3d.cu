@@ -82,8 +82,8 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (uint32_t i = 0; i < kTcSpin; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint32_t limit = kTcSpin) {
+  for (uint32_t i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
@@ -539,6 +539,31 @@ int xac_conv3d_weight_grad(const void* in, int N, int D, int H, int W, int Ci, c
     bias_grad_final_kernel<<<1, Co, 0, st>>>(partial, kBiasBlocks, Co, db);
   }
   XAC_CUDA(cudaGetLastError());
+  return XAC_OK;
+}
+
+// Test-only: the convolution kernels' mbarrier wait on a barrier that nothing completes must give up after
+// `limit` polls and set g_conv_status (read and cleared by xac_conv3d_status).
+static __global__ void test_conv_wait_timeout_kernel(uint32_t limit) {
+  __shared__ __align__(8) uint64_t bar;
+  const uint32_t b = smem_addr(&bar);
+  if (threadIdx.x == 0) {
+    mbar_init(b, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_wait(b, 0, limit);
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(b) : "memory");
+  }
+}
+
+int xac_test_conv_wait_timeout(unsigned limit, void* stream) {
+  XAC_REQUIRE(limit > 0 && limit <= (1u << 20), "xac_test_conv_wait_timeout: limit %u out of (0, 2^20]", limit);
+  cudaStream_t s = as_stream(stream);
+  test_conv_wait_timeout_kernel<<<1, 32, 0, s>>>(limit);
+  XAC_CUDA(cudaGetLastError());
+  XAC_CUDA(cudaStreamSynchronize(s));
   return XAC_OK;
 }
 
