@@ -137,10 +137,29 @@ struct Rows {
     return b + (I * T - ex_of(I) - ey_of(I) * kQ * T);
   }
 };
+// Runtime row length: one base pointer and 32-bit element indices (every index of a population array fits in 31
+// bits), so an address is formed right before its load instead of 19 64-bit pointers living at once.
+template <typename S>
+struct Rows<S, 0> {
+  const S* base;
+  uint32_t c, zm, zp;
+  int RL;
+  __device__ __forceinline__ const S* own(int i) const { return base + (c + (uint32_t)(i * RL)); }
+  template <int I>
+  __device__ __forceinline__ const S* pull() const {
+    const uint32_t b = ez_of(I) > 0 ? zm : (ez_of(I) < 0 ? zp : c);
+    return base + (b + (uint32_t)((I - ey_of(I) * kQ) * RL - ex_of(I)));
+  }
+};
 template <int kT, typename S>
 __device__ __forceinline__ Rows<S, kT> rows_at(const S* base, uint32_t e0, const Geom& g, int pitch) {
-  const long long slab = (long long)g.ny * kQ * pitch;
-  return {base + e0, base + e0 - slab, base + e0 + slab, pitch};
+  if constexpr (kT > 0) {
+    const long long slab = (long long)g.ny * kQ * pitch;
+    return {base + e0, base + e0 - slab, base + e0 + slab, pitch};
+  } else {
+    const uint32_t slab = (uint32_t)g.ny * kQ * (uint32_t)pitch;
+    return {base, e0, e0 - slab, e0 + slab, pitch};
+  }
 }
 
 #define XAC_FOR19(M) M(0) M(1) M(2) M(3) M(4) M(5) M(6) M(7) M(8) M(9) M(10) M(11) M(12) M(13) M(14) M(15) M(16) M(17) M(18)
