@@ -355,13 +355,17 @@ def run_gpu_arm(args):
     # path (kernel modules of the stats and run-loop code, host staging buffers of the field read-back)
     run_simulation(mask, max_steps=2 * STEPS_PER_BENCH_STEP + 1, tau_fluid=TAU, heat_power=POWER, u_inlet_val=u_in,
                    heat_source=hs, tol_ke=TOL, tol_T=TOL, Pr=PR, k_ratio=K_RATIO, silent=True, device=str(dev))
-    barrier(world)
-    torch.cuda.synchronize(dev)
-    t = time.perf_counter()
-    res = run_simulation(mask, max_steps=MAX_STEPS, tau_fluid=TAU, heat_power=POWER, u_inlet_val=u_in,
-                         heat_source=hs, tol_ke=TOL, tol_T=TOL, Pr=PR, k_ratio=K_RATIO, silent=True,
-                         device=str(dev))
-    e2e_s = time.perf_counter() - t
+    # three timed solves (the host's share varies between runs on a shared machine): the median is reported
+    solve_s = []
+    for _ in range(3):
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        t = time.perf_counter()
+        res = run_simulation(mask, max_steps=MAX_STEPS, tau_fluid=TAU, heat_power=POWER, u_inlet_val=u_in,
+                             heat_source=hs, tol_ke=TOL, tol_T=TOL, Pr=PR, k_ratio=K_RATIO, silent=True,
+                             device=str(dev))
+        solve_s.append(time.perf_counter() - t)
+    e2e_s = sorted(solve_s)[1]
     e2e_max = max_over_ranks(e2e_s, world)
     e2e_lups = sum_over_ranks(cells * res["steps"], world)
     e2e_value = e2e_lups / e2e_max / 1e6
@@ -396,6 +400,7 @@ def run_gpu_arm(args):
                              "alg_bytes_per_launch": alg_bytes, "mean_launch_us": round(step_ms * 1e3, 3)},
                 "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "s_per_solve": round(e2e_max, 4),
+                        "solves_s": [round(x, 4) for x in solve_s],
                         "solver_steps": res["steps"], "converged": res["converged"]},
                 "gpu_launches": args.steps * (STEPS_PER_BENCH_STEP + 3),
                 "launch_shape": {"block": shape["block"], "variant": shape["variant"], "autotuned": shape["table"]},
