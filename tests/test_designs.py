@@ -64,3 +64,40 @@ def test_straight_fin_plate_layout():
     assert m.shape == (64, 32, 16)
     assert (m[8:56, 4:6, 4:15] == 1).all() and (m[8:56, 6:9, 4:15] == 0).all()
     assert (m[0, 1:31, 4:15] == 2).all() and (m[63, 1:31, 4:15] == 3).all()
+
+
+def _evaluate_spec(spec):
+    """The per-cell rule of the device design kernel (csrc/designs.cu), restated in numpy for the parameters
+    reference_spec produces: the same inputs must give the reference's masks without a GPU."""
+    nx, ny, nz = spec["shape"]
+    buf = spec["buf"]
+    core = nx - 2 * buf
+    p0, p1 = spec["p"]
+    solid = np.zeros((core, ny, nz), dtype=bool)
+    fam = spec["family"]
+    if fam == "straight":
+        designs._straight_channels(solid, int(p0), int(p1))
+    elif fam == "pin_fin":
+        X, Y = np.meshgrid(np.arange(core), np.arange(ny), indexing="ij")
+        h, ip = p1 / 2, int(p1)
+        da = ((X % ip) - h) ** 2 + ((Y % ip) - h) ** 2
+        db = (np.mod(X - h, p1) - h) ** 2 + (np.mod(Y - h, p1) - h) ** 2
+        solid[:] = (np.minimum(da, db) < p0 * p0)[:, :, None]
+    elif fam in ("gyroid", "schwarz_p", "schwarz_d"):
+        kind = {"gyroid": 3, "schwarz_p": 4, "schwarz_d": 5}[fam]
+        f = designs.tpms_field(kind, (core, ny, nz), p0)
+        solid[:] = (f < p1) if spec.get("below") else (f > p1)
+        m = spec.get("margin", 0)
+        if m:
+            solid[:m] = False
+            solid[-m:] = False
+    mask = np.zeros((nx, ny, nz), dtype=np.int32)
+    mask[buf:buf + core][solid] = designs.BC_SOLID
+    return designs._frame(mask)
+
+
+@pytest.mark.parametrize("case", D["masks"], ids=lambda c: "t{design_type}-{feature_size}-{spacing}".format(**c["state"]))
+def test_reference_spec_reproduces_the_reference_masks(case):
+    """reference_spec's parameters (what the device builder evaluates) give the reference's mask bytes."""
+    m = _evaluate_spec(designs.reference_spec(case["state"]))
+    assert sha(m.astype(np.int32)) == case["sha256"]
