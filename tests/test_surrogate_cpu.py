@@ -92,3 +92,17 @@ def test_trained_weights_load_and_run_cpu():
     x[..., 2] = 0.6
     y = m.forward(x.to(S.BF16), S.torch_conv3d)
     assert y.shape == (1, 8, 16, 24, 16) and torch.isfinite(y).all()
+
+
+def test_comparison_against_a_tight_solve():
+    """warmstart._vs: relative delta_P / R_th differences over the designs converged in both batches, and the
+    count within 0.5% on both."""
+    from xadvcool_b200 import warmstart as W
+    ref = {"scalars": [{"delta_P": 1.0, "R_th": 2.0}, {"delta_P": 1.0, "R_th": 2.0}, {"delta_P": 1.0, "R_th": 2.0}]}
+    a = {"scalars": [{"delta_P": 1.001, "R_th": 2.002}, {"delta_P": 1.0, "R_th": 2.1}, {"delta_P": 5.0, "R_th": 9.0}]}
+    r = W._vs(a, ref, [True, True, False], [True, True, True])
+    assert r["compared"] == 2
+    assert abs(r["dP_rel_max"] - 1e-3) < 1e-12
+    assert abs(r["Rth_rel_max"] - 0.05) < 1e-12
+    assert r["within_half_percent"] == 1
+    assert W._vs(a, ref, [False] * 3, [True] * 3)["compared"] == 0
