@@ -106,3 +106,14 @@ def test_comparison_against_a_tight_solve():
     assert abs(r["Rth_rel_max"] - 0.05) < 1e-12
     assert r["within_half_percent"] == 1
     assert W._vs(a, ref, [False] * 3, [True] * 3)["compared"] == 0
+
+
+def test_convolution_kernels_refuse_host_tensors():
+    """Host tensors are refused before any pointer reaches the library."""
+    import pytest
+    x = torch.zeros((1, 2, 2, 2, 16), dtype=torch.bfloat16)
+    w = torch.zeros((27, 16, 16), dtype=torch.bfloat16)
+    with pytest.raises(ValueError, match="CUDA tensor"):
+        S.conv_forward(x, w, None, 3)
+    with pytest.raises(ValueError, match="CUDA tensor"):
+        S.conv_weight_grad(x, x, 3, False)

@@ -35,9 +35,24 @@ def _pad16(c):
 
 
 # ------------------------------------------------------------------------------------------------ kernels
+def _on_one_gpu(**tensors) -> None:
+    """The convolution kernels take raw device pointers: every operand must be a CUDA tensor of one device (a host
+    tensor would hand the kernel a host address)."""
+    dev = None
+    for name, t in tensors.items():
+        if t is None:
+            continue
+        if not isinstance(t, torch.Tensor) or not t.is_cuda:
+            raise ValueError(f"{name}: the convolution kernels need a CUDA tensor (there is no CPU path)")
+        if dev is not None and t.device != dev:
+            raise ValueError(f"{name}: on {t.device}, the other operands are on {dev}")
+        dev = t.device
+
+
 def conv_forward(x: torch.Tensor, w_bf: torch.Tensor, bias: torch.Tensor | None, ksize: int, act: int = 0,
                  out_fp32: bool = False) -> torch.Tensor:
     """x: [N,D,H,W,Ci] bf16; w_bf: [taps,Co,Ci] bf16; bias fp32 [Co] or None -> [N,D,H,W,Co]."""
+    _on_one_gpu(x=x, w=w_bf, bias=bias)
     N, D, H, W, Ci = x.shape
     taps, Co, Ci_w = w_bf.shape
     assert Ci_w == Ci and taps == (27 if ksize == 3 else 1)
@@ -50,6 +65,7 @@ def conv_forward(x: torch.Tensor, w_bf: torch.Tensor, bias: torch.Tensor | None,
 
 
 def conv_weight_grad(x: torch.Tensor, dy: torch.Tensor, ksize: int, with_bias: bool):
+    _on_one_gpu(x=x, dy=dy)
     N, D, H, W, Ci = x.shape
     Co = dy.shape[-1]
     taps = 27 if ksize == 3 else 1
