@@ -28,6 +28,7 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parent.parent))  # the repository root: oracle/ and xadvcool_b200/
 
 
 def synthetic_fields(seed: int, shape=(148, 128, 32)):
