@@ -122,3 +122,38 @@ def test_batch_tile_autotune(cuda, tmp_path, monkeypatch):
         for a, c in zip((t.cpu().numpy() for t in b.lattice(i).fields()), f_ref):
             assert np.array_equal(a, c)
     b.close()
+
+
+C4_SEEDS = (0, 1, 2, 4, 6, 7, 9, 10, 18)  # every x in {96,128,148,192}, y in {64,96,128}, z in {16,32,48}, 5 families
+
+
+def c4_designs():
+    out = []
+    for s in C4_SEEDS:
+        m, hs, u, info = designs.mixed_design(s)
+        out.append(dict(mask=m, heat_source=hs, tau_fluid=0.56, u_inlet_val=u, Pr=7.0, k_ratio=628.0,
+                        heat_power=0.1))
+    out[7] = dict(out[7], u_inlet_val=0.3, tau_fluid=0.51)  # 148x64x16 straight channel: retires by divergence
+    return out
+
+
+def test_batch_of_dataset_shapes_equals_solo_solves(cuda):
+    """Nine designs of the batching workload's shapes and families (up to 192x96x32 and 148x96x48, 3.3 M cells) in
+    one persistent launch, retiring at different steps by convergence or divergence: each design's step count,
+    flags, convergence rates and fields equal its solo solve bit for bit."""
+    ds = c4_designs()
+    run = dict(max_steps=2000, stats_every=100, tol_ke=1e-3, tol_T=1e-3, min_steps=200)
+    b = Batch(ds)
+    res = b.run(**run)
+    steps = [r["steps"] for r in res]
+    print("batch steps:", steps)
+    for i, d in enumerate(ds):
+        ref, f_ref = solo(d, **run)
+        assert res[i]["steps"] == ref["steps"], (i, res[i]["steps"], ref["steps"])
+        assert res[i]["converged"] == ref["converged"] and res[i]["diverged"] == ref["diverged"]
+        assert res[i]["d_ke"] == ref["d_ke"] and res[i]["dQ_conv"] == ref["dQ_conv"]
+        for a, c in zip((t.cpu().numpy() for t in b.lattice(i).fields()), f_ref):
+            assert np.array_equal(a.view(np.uint32), c.view(np.uint32))  # bit patterns: the diverged one holds NaN
+    assert res[7]["diverged"] and any(r["converged"] for r in res)
+    assert len(set(steps)) >= 3  # retirement interleaves
+    b.close()

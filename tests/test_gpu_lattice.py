@@ -50,6 +50,16 @@ def assert_exact(ref, rho, u, T):
         assert np.array_equal(a, b), f"{name}: {np.count_nonzero(d)} cells differ, max |diff| {d.max():.3e}"
 
 
+def test_benchmark_gyroid_148x128x32_300_steps_bit_exact(cuda):
+    """The benchmarked state itself: the seed-0 gyroid at full size (606,208 cells, 57% solid, Pr 7, k_ratio 628,
+    tau 0.55, heat power 0.1) after 300 coupled steps, in the launch shape the step uses by default."""
+    mask, hs, u_in, _ = designs.gyroid_design(0)
+    kw = dict(tau_fluid=0.55, u_inlet_val=u_in, Pr=7.0, k_ratio=628.0, heat_power=0.1)
+    ref = oracle_fields(mask, 300, hs=hs, **kw)
+    _, rho, u, T = lattice_fields(mask, 300, hs=hs, **kw)
+    assert_exact(ref, rho, u, T)
+
+
 def test_config1_straight_fin_plate_2000_steps_bit_exact(cuda):
     mask = designs.straight_fin_plate()
     ref = oracle_fields(mask, 2000, **C1)
@@ -67,8 +77,9 @@ def test_random_channel_step_chunking_bit_exact(chunks, cuda):
     assert_exact(ref, rho, u, T)
 
 
-@pytest.mark.parametrize("shape", [(3, 3, 3), (5, 1, 1), (40, 3, 17), (17, 33, 5)])
+@pytest.mark.parametrize("shape", [(3, 3, 3), (5, 1, 1), (40, 3, 17), (17, 33, 5), (33, 6, 5), (64, 5, 4)])
 def test_ragged_and_tiny_lattices(shape, cuda):
+    """Random labels: inlet and outlet cells anywhere (even and odd x, next to solids), odd and even row lengths."""
     rng = np.random.default_rng(sum(shape))
     mask = rng.choice([0, 0, 1, 2, 3], size=shape).astype(np.int32)
     kw = dict(tau_fluid=0.7, heat_power=1e-2, u_inlet_val=0.02, Pr=1.5, k_ratio=10.0)
@@ -223,10 +234,11 @@ def test_launch_shapes_give_identical_bits(precision, block, cuda):
 
 
 @pytest.mark.parametrize("variant", [0, 1])
-@pytest.mark.parametrize("nx", [20, 33, 100, 150, 300])
+@pytest.mark.parametrize("nx", [20, 33, 90, 100, 150, 180, 220, 250, 300])
 def test_row_lengths_match_oracle(nx, variant, cuda):
-    """Row lengths 32, 64, 128, 160 (compile-time) and 320 (runtime pitch), ragged x padding, both visiting orders
-    (the staged one falls back to one thread per row position below 64 and above 256): bit-exact FP32."""
+    """Every compiled row length: 32, 64, 96, 128, 160, 192, 224, 256, and 320 (runtime pitch), with ragged x
+    padding, in both visiting orders (the staged one falls back to one thread per row position below 64 and above
+    256): bit-exact FP32."""
     mask, hs, u_in, _ = designs.gyroid_design(5, nx=nx, ny=9, nz=7, buf=4)
     kw = dict(heat_source=hs, tau_fluid=0.57, u_inlet_val=min(u_in, 0.04), heat_power=0.05)
     lat = Lattice(mask, **kw)
@@ -288,3 +300,32 @@ def test_16bit_storage_scalar_errors(cuda):
     for p, b in bounds.items():
         for k, lim in zip(keys, b):
             assert rel[p][k] < lim, (p, k, rel[p][k])
+
+
+def _rel_l2(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+@pytest.mark.parametrize("precision", ["fp16", "bf16"])
+@pytest.mark.parametrize("nx", [150, 180])
+def test_16bit_storage_at_row_lengths_160_and_192(nx, precision, cuda):
+    """16-bit storage on a gyroid at row lengths 160 and 192 (the benchmark and dataset widths): both visiting orders
+    give the same bits, and the fields stay close to FP32 storage after 300 steps."""
+    mask, hs, u_in, _ = designs.gyroid_design(6, nx=nx, ny=12, nz=8, buf=4)
+    kw = dict(heat_source=hs, tau_fluid=0.57, u_inlet_val=min(u_in, 0.04), heat_power=0.05)
+    out = {}
+    for prec, v in ((precision, 0), (precision, 1), ("fp32", 0)):
+        lat = Lattice(mask, precision=prec, **kw)
+        lat.tune(128, v)
+        lat.step(300)
+        out[(prec, v)] = [t.cpu().numpy() for t in lat.fields()]
+        lat.close()
+    for a, b in zip(out[(precision, 0)], out[(precision, 1)]):
+        assert np.array_equal(a, b)
+    (rho, u, T), (r32, u32, T32) = out[(precision, 0)], out[("fp32", 0)]
+    fl = mask != 1
+    e_u, e_p, e_T = _rel_l2(u[fl], u32[fl]), _rel_l2(rho[fl] - 1.0, r32[fl] - 1.0), _rel_l2(T - 25.0, T32 - 25.0)
+    print(f"{precision} nx={nx}: rel L2 vs FP32 u {e_u:.3e} p {e_p:.3e} T {e_T:.3e}")
+    lim = {"fp16": (2e-2, 5e-2), "bf16": (1e-1, 0.5)}[precision]
+    assert e_u < lim[0] and e_p < lim[0] and e_T < lim[1]
