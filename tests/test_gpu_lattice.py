@@ -327,5 +327,7 @@ def test_16bit_storage_at_row_lengths_160_and_192(nx, precision, cuda):
     fl = mask != 1
     e_u, e_p, e_T = _rel_l2(u[fl], u32[fl]), _rel_l2(rho[fl] - 1.0, r32[fl] - 1.0), _rel_l2(T - 25.0, T32 - 25.0)
     print(f"{precision} nx={nx}: rel L2 vs FP32 u {e_u:.3e} p {e_p:.3e} T {e_T:.3e}")
-    lim = {"fp16": (2e-2, 5e-2), "bf16": (1e-1, 0.5)}[precision]
-    assert e_u < lim[0] and e_p < lim[0] and e_T < lim[1]
+    # measured on B200 (both row lengths): fp16 u 8.1e-4, p 2.5e-3, T 1.6e-3; bf16 u 6.5e-3, p 1.5e-3, T 1.3e-2.
+    # Bounds: about 2x those.
+    lim = {"fp16": (2e-3, 5e-3, 4e-3), "bf16": (1.5e-2, 4e-3, 3e-2)}[precision]
+    assert e_u < lim[0] and e_p < lim[1] and e_T < lim[2]
