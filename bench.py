@@ -70,13 +70,33 @@ def hbm_peak():
     return 6650.0, "fallback"
 
 
-def ncu_traffic_per_cell():
-    """Per-cell-step DRAM bytes of the fused step from the committed ncu summary, if present."""
+STEP_SOURCES = ("xac_internal.cuh", "lattice_kernels.cuh", "step_kernels.cuh", "step_f32.cu")
+
+
+def step_sources_sha256():
+    """SHA-256 over the sources of the FP32 fused step kernel (the file contents, in a fixed order)."""
+    import hashlib
+    h = hashlib.sha256()
+    for name in STEP_SOURCES:
+        h.update((ROOT / "xadvcool_b200" / "csrc" / name).read_bytes())
+    return h.hexdigest()
+
+
+def ncu_traffic_per_cell(block, variant):
+    """Per-cell-step DRAM bytes of the fused step for this launch shape from the committed ncu summary, and why it
+    is None: the summary names the kernel sources it was captured from (SHA-256) and one figure per launch shape,
+    so a figure from other sources or another shape is never reported."""
     p = ROOT / "profiles" / "coupled_step_gyroid148.md"
     if not p.exists():
-        return None
-    m = re.search(r"dram_bytes_per_cell_step:\s*([0-9.]+)", p.read_text())
-    return float(m.group(1)) if m else None
+        return None, "no committed profile"
+    text = p.read_text()
+    m = re.search(r"profiled_sources_sha256:\s*([0-9a-f]{64})", text)
+    if not m or m.group(1) != step_sources_sha256():
+        return None, "the committed profile was captured from other step kernel sources"
+    m = re.search(rf"dram_bytes_per_cell_step\[block={block},variant={variant}\]:\s*([0-9.]+)", text)
+    if not m:
+        return None, f"the committed profile has no figure for block {block}, variant {variant}"
+    return float(m.group(1)), None
 
 
 # ------------------------------------------------------------------------------------------------ clocks
@@ -237,6 +257,79 @@ def run_reference_arm(args):
 
 # ------------------------------------------------------------------------------------------------ GPU
 STEP_KERNELS = {0: "coupled_step_kernel<float>", 1: "coupled_qstage_kernel<float>"}
+# The first of the benchmark gyroid seeds 0-23 whose cold solve reaches residual 1e-6 within 30000 steps (19,800
+# steps; seed 0 stops at the step limit, 11 of the 24 trip the divergence guard at the first check).
+CONVERGED_SEED = 15
+
+
+def converged_e2e(dev):
+    """One cold run_simulation of a benchmark-family gyroid that converges, host numpy in and out (after the seed-0
+    solves have loaded every module): seconds per converged design and its MLUPS."""
+    from xadvcool_b200.simulation import run_simulation
+    mask, hs, u_in, info = workload(CONVERGED_SEED)
+    torch_sync(dev)
+    t = time.perf_counter()
+    res = run_simulation(mask, max_steps=MAX_STEPS, tau_fluid=TAU, heat_power=POWER, u_inlet_val=u_in, heat_source=hs,
+                         tol_ke=TOL, tol_T=TOL, Pr=PR, k_ratio=K_RATIO, silent=True, device=str(dev))
+    dt = time.perf_counter() - t
+    return {"design": info, "s_per_solve": round(dt, 4), "steps": res["steps"], "converged": res["converged"],
+            "mlups": round(mask.size * res["steps"] / dt / 1e6, 1)}
+
+
+def torch_sync(dev):
+    import torch
+    torch.cuda.synchronize(dev)
+
+
+def c4_probe(dev, tol=TOL):
+    """The batching workload as specified: 64 seeded designs of the five families (x in {96,128,148,192}, y in
+    {64,96,128}, z in {16,32,48}), FP32, each solved to residual ``tol`` (at most 30000 steps, the reference's
+    convergence rule): one persistent batch (autotuned tile, graph-captured launches) against the same designs
+    solved one after another by the single-lattice run loop. Each side is timed from lattice creation (mask
+    upload) to the last design's scalars; seconds per converged design = wall time / designs that converged."""
+    from xadvcool_b200 import autotune, designs
+    from xadvcool_b200.batch import Batch
+    from xadvcool_b200.lattice import Lattice
+    ds = []
+    for s in range(64):
+        m, h, u, _ = designs.mixed_design(s)
+        ds.append(dict(mask=m, heat_source=h, tau_fluid=0.56, u_inlet_val=u))
+    run = dict(max_steps=MAX_STEPS, stats_every=100, tol_ke=tol, tol_T=tol)
+
+    def scal(lat, m):
+        return lat.scalars(buf=10, core_nx=m.shape[0] - 20, core_ny=m.shape[1])
+
+    tile = autotune.autotune_batch(ds, device=dev)  # cached: forms_probe timed the tiles of this design set
+    torch_sync(dev)
+    t = time.perf_counter()
+    with Batch(ds, device=dev) as b:
+        b.tune(tile["block"], b.get_tune()[1])
+        res_b = b.run(**run)
+        sc_b = [scal(b.lattice(i), d["mask"]) for i, d in enumerate(ds)]
+        launches = b.launch_counts()
+    torch_sync(dev)
+    t_b = time.perf_counter() - t
+    t = time.perf_counter()
+    res_s, sc_s = [], []
+    for d in ds:
+        with Lattice(d["mask"], device=dev, **{k: v for k, v in d.items() if k != "mask"}) as lat:
+            res_s.append(lat.run(**run))
+            sc_s.append(scal(lat, d["mask"]))
+    torch_sync(dev)
+    t_s = time.perf_counter() - t
+    conv_b = sum(r["converged"] for r in res_b)
+    conv_s = sum(r["converged"] for r in res_s)
+    lups = sum(d["mask"].size * r["steps"] for d, r in zip(ds, res_b))
+    same = all(a["steps"] == c["steps"] and x["delta_P"] == y["delta_P"] and x["R_th"] == y["R_th"]
+               for a, c, x, y in zip(res_b, res_s, sc_b, sc_s))
+    return {"designs": len(ds), "tol": tol, "max_steps": MAX_STEPS, "tile": tile["block"],
+            "converged": conv_b, "diverged": sum(r["diverged"] for r in res_b),
+            "at_step_limit": sum(not r["converged"] and not r["diverged"] for r in res_b),
+            "batched_s": round(t_b, 3), "solo_s": round(t_s, 3),
+            "batched_s_per_converged_design": round(t_b / max(conv_b, 1), 4),
+            "solo_s_per_converged_design": round(t_s / max(conv_s, 1), 4),
+            "batched_over_solo": round(t_s / t_b, 3), "batched_mlups": round(lups / t_b / 1e6, 1),
+            "batch_equals_solo": same, "graph_launches": launches[0], "direct_launches": launches[1]}
 
 
 def warm_start_probe(n_designs=16, tol=TOL):
@@ -291,10 +384,12 @@ def forms_probe(dev, mask, lat_kw, shape):
     b.run(max_steps=1000, stats_every=100, tol_ke=0.0, tol_T=0.0)
     torch.cuda.synchronize(dev)
     dt = time.perf_counter() - t
+    out["batch64_launches"] = dict(zip(("graph", "direct"), b.launch_counts()))
     b.close()
     out["batch64_mixed_mlups"] = round(cells * 1000 / dt / 1e6, 1)
     out["batch64_cells"] = cells
     out["batch64_tile"] = {"block": tiles["block"], "autotuned_us_per_step": tiles["table"]}
+    out["c4_to_convergence"] = c4_probe(dev)
     out["warm_start"] = warm_start_probe()
     return out
 
@@ -355,7 +450,9 @@ def run_gpu_arm(args):
     alg_bytes = 152.0 * cells + 152.0 * (cells - n_solid)  # thermal r+w every cell, fluid r+w non-solid
     achieved = alg_bytes / (step_ms * 1e-3) / 1e9
     peak, peak_kind = hbm_peak()
-    tpc = ncu_traffic_per_cell()
+    tpc, tpc_why = ncu_traffic_per_cell(shape["block"], shape["variant"])
+    # the floor of the step's memory access pattern on this design: the same loads and stores, no arithmetic
+    pattern_us = lat.pattern_copy_us(launches=5 * STEPS_PER_BENCH_STEP)
     lat.close()
 
     # e2e: a full solve through the public API, host numpy in and out; one short untimed solve first warms the
@@ -382,6 +479,7 @@ def run_gpu_arm(args):
     h2d = mask.size * 4 + hs.size * 4 + 272
     d2h = cells * 5 * 4 + 17 * 8 + 272
 
+    conv_e2e = converged_e2e(dev) if rank == 0 else None
     # side measurements of the other forms, after the headline numbers (they load the GPU heavily)
     forms = forms_probe(dev, mask, lat_kw, shape) if rank == 0 else None
 
@@ -401,15 +499,22 @@ def run_gpu_arm(args):
                 "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                              "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                              "traffic": (round(tpc * cells) if tpc else None),
-                             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch inside "
-                                               "the 100-step loop (L2 as the previous step left it), "
-                                               "profiles/coupled_step_gyroid148.md",
+                             "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per launch inside "
+                                                "the 100-step loop (L2 as the previous step left it), this launch "
+                                                "shape, the same kernel sources (SHA-256), "
+                                                "profiles/coupled_step_gyroid148.md" if tpc else tpc_why),
                              "kernel": STEP_KERNELS[shape["variant"]],
-                             "alg_bytes_per_launch": alg_bytes, "mean_launch_us": round(step_ms * 1e3, 3)},
+                             "alg_bytes_per_launch": alg_bytes, "mean_launch_us": round(step_ms * 1e3, 3),
+                             "pattern_floor": {"us_per_launch": round(pattern_us, 3),
+                                               "step_frac": round(pattern_us / (step_ms * 1e3), 4),
+                                               "what": "the step's loads and stores (same addresses, solid "
+                                                       "skips, sector fills) with no arithmetic, timed on the "
+                                                       "same lattice: step_frac = floor / step time"}},
                 "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "s_per_solve": round(e2e_max, 4),
                         "solves_s": [round(x, 4) for x in solve_s],
-                        "solver_steps": res["steps"], "converged": res["converged"]},
+                        "solver_steps": res["steps"], "converged": res["converged"],
+                        "converged_design": conv_e2e},
                 "gpu_launches": args.steps * (STEPS_PER_BENCH_STEP + 3),
                 "launch_shape": {"block": shape["block"], "variant": shape["variant"], "autotuned": shape["table"]},
                 "forms": forms,

@@ -213,10 +213,23 @@ int xac_lattice_steps_done(const xac_lattice *lat, long long *steps);
 /* Launch shape of the fused step kernel: threads per block (64, 128, 256) and the visiting order:
  * variant 0 = one thread per row position, in memory order; variant 1 = one block per row whose thermal input is
  * staged in shared memory by bulk copies while the fluid lattice runs (row lengths 64..256; other lengths run
- * variant 0). Results do not depend on the shape (every cell runs the same arithmetic); xadvcool_b200.autotune
- * picks it. */
+ * variant 0). Variant 1 waits for its copies with a bounded wait; if a wait ever gives up, the call that sees it
+ * (xac_lattice_stats, xac_lattice_run) returns XAC_ETIMEOUT and the lattice refuses every further step, run, stats,
+ * fields, scalars, validate and save-state call with XAC_ETIMEOUT until xac_lattice_init_fields or
+ * xac_lattice_load_state rewrites its populations. Results do not depend on the shape (every cell runs the same
+ * arithmetic); xadvcool_b200.autotune picks it. */
 int xac_lattice_tune(xac_lattice *lat, int block, int variant);
 int xac_lattice_get_tune(const xac_lattice *lat, int *block, int *variant);
+/* Diagnostic, no reference counterpart: the floor that the fused step's memory access pattern sets for this
+ * lattice. Times `launches` launches of a kernel with the step's threads (the lattice's block size, one thread per
+ * row position, the alternating sweep), link-word reads, population addresses (fluid pulls with the bounce-back
+ * reads, thermal pulls, solid cells' fluid populations skipped, whole-sector fills) and no arithmetic: each value
+ * read is stored unchanged. CUDA events on `stream`, after 4 untimed launches. The copies are not a physical state,
+ * so the lattice is re-initialised to the cold start (step 0) afterwards. */
+int xac_lattice_pattern_copy(xac_lattice *lat, int launches, double *us_per_launch, void *stream);
+/* Test hook: writes the lattice's step status word as a staged step kernel whose wait gave up would (no kernel
+ * runs), so that a test sees the lattice refuse work and recover after xac_lattice_init_fields. */
+int xac_test_set_step_status(xac_lattice *lat, unsigned value, void *stream);
 /* Inputs of generate_dataset.py:80 compute_macroscopic_metrics that are not fields. */
 typedef struct xac_scalar_params {
     int buf;            /* inlet/outlet buffer length along x (10, generate_dataset.py:90)            */
@@ -358,6 +371,28 @@ int xac_batch_get_tune(const xac_batch *batch, int *block, int *steps_per_launch
  * outcome. With opts->constant_power the reference's pump controller (simulation.py:139-146) runs inside the
  * persistent kernel on each design's stats, exactly as xac_lattice_run runs it for one lattice. */
 int xac_batch_run(xac_batch *batch, const xac_run_opts *opts, xac_run_result *results, void *stream);
+/* Persistent launches of this batch so far: from a captured CUDA graph, and direct (cooperative) launches, which
+ * are used when the driver cannot capture the cooperative launch and for launches shorter than steps_per_launch. */
+int xac_batch_launch_counts(const xac_batch *batch, long long *graph_launches, long long *direct_launches);
+
+/* Open batch: a design sweep (generate_dataset.py:365-436, one solve per design there) as a queue over one
+ * persistent kernel. xac_batch_open makes an empty batch of one precision. xac_batch_admit creates a design in a
+ * free slot (at most 1024 slots; a released slot is reused); it joins the running batch at the next multiple of
+ * opts->stats_every of the batch's step count, from its own step 0, so every design keeps exactly the steps,
+ * decisions and bits of its solo xac_lattice_run. xac_batch_advance runs the batch for up to `steps` steps, and
+ * returns early after the launch in which designs finish (so that their slots can be refilled) or when no design
+ * is left; it reports the designs that finished during the call (converged,
+ * diverged, or at opts->max_steps of their own): their slots, outcomes, and the wall seconds of the launches they
+ * took part in, shared among the designs of each launch in proportion to their cells. slots / results /
+ * gpu_seconds must hold xac_batch_size() entries. A finished design keeps its lattice (xac_batch_lattice: fields,
+ * stats, scalars) until xac_batch_release frees its slot and device memory. xac_lattice_footprint gives the
+ * device bytes a design will take, for admission under a memory budget. */
+int xac_batch_open(int precision, xac_batch **out);
+int xac_batch_admit(xac_batch *batch, const xac_desc *design, int *slot, void *stream);
+int xac_batch_advance(xac_batch *batch, const xac_run_opts *opts, long long steps, int *n_finished, int *slots,
+                      xac_run_result *results, double *gpu_seconds, void *stream);
+int xac_batch_release(xac_batch *batch, int slot);
+int xac_lattice_footprint(const xac_desc *design, unsigned long long *bytes);
 
 #ifdef __cplusplus
 }

@@ -15,12 +15,13 @@ does not, so the outputs are committed).
                   every failed id among them) and hashing each parameter set into its sample id as
                   generate_dataset.py:368-369 does. Solved designs exclude gaussian_hotspots heat maps.
 
-Usage: python tests/golden/make_golden.py [/path/to/reference]
+Usage: python tests/golden/make_golden.py REFERENCE_DIR   (or XAC_REFERENCE_DIR=REFERENCE_DIR)
 """
 from __future__ import annotations
 
 import hashlib
 import json
+import os
 import sys
 import types
 from pathlib import Path
@@ -251,4 +252,8 @@ def main(ref: Path):
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    ref_dir = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("XAC_REFERENCE_DIR")
+    if not ref_dir:
+        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_DIR  (or set XAC_REFERENCE_DIR): the path of "
+                 "the reference checkout whose geometry, metrics and validator code generate the fixtures")
+    main(Path(ref_dir))

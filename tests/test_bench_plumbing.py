@@ -9,11 +9,28 @@ sys.path.insert(0, str(ROOT))
 import bench  # noqa: E402
 
 
-def test_traffic_comes_from_the_committed_profile():
+def test_traffic_comes_from_the_committed_profile_of_the_same_kernel_and_shape():
     text = (ROOT / "profiles" / "coupled_step_gyroid148.md").read_text()
-    assert "dram_bytes_per_cell_step:" in text
-    tpc = bench.ncu_traffic_per_cell()
-    assert tpc is not None and 150.0 < tpc < 320.0  # between the solid-aware and the all-cell algorithmic bytes
+    assert f"profiled_sources_sha256: {bench.step_sources_sha256()}" in text
+    for block in (64, 128, 256):
+        tpc, why = bench.ncu_traffic_per_cell(block, 0)
+        assert why is None and 150.0 < tpc < 320.0  # between the solid-aware and the all-cell algorithmic bytes
+    tpc, why = bench.ncu_traffic_per_cell(96, 0)
+    assert tpc is None and "no figure" in why
+
+
+def test_traffic_is_withheld_for_other_kernel_sources(tmp_path, monkeypatch):
+    prof = tmp_path / "profiles"
+    prof.mkdir()
+    text = (ROOT / "profiles" / "coupled_step_gyroid148.md").read_text()
+    (prof / "coupled_step_gyroid148.md").write_text(text.replace(bench.step_sources_sha256(), "0" * 64))
+    src = tmp_path / "xadvcool_b200" / "csrc"
+    src.mkdir(parents=True)
+    for name in bench.STEP_SOURCES:
+        (src / name).write_bytes((ROOT / "xadvcool_b200" / "csrc" / name).read_bytes())
+    monkeypatch.setattr(bench, "ROOT", tmp_path)
+    tpc, why = bench.ncu_traffic_per_cell(128, 0)
+    assert tpc is None and "other step kernel sources" in why
 
 
 def test_peak_is_measured_or_the_stated_fallback(tmp_path, monkeypatch):

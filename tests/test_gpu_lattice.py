@@ -331,3 +331,22 @@ def test_16bit_storage_at_row_lengths_160_and_192(nx, precision, cuda):
     # Bounds: about 2x those.
     lim = {"fp16": (2e-3, 5e-3, 4e-3), "bf16": (1.5e-2, 4e-3, 3e-2)}[precision]
     assert e_u < lim[0] and e_p < lim[1] and e_T < lim[2]
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp16"])
+def test_pattern_copy_probe_times_and_restarts_the_lattice(precision, cuda):
+    """The memory-pattern probe returns a positive time per launch, and leaves the lattice at the cold start: the
+    next steps give the same bits as a fresh lattice's."""
+    mask, hs, u_in, _ = designs.gyroid_design(4, nx=70, ny=20, nz=12, buf=4)
+    kw = dict(heat_source=hs, tau_fluid=0.57, u_inlet_val=min(u_in, 0.04), heat_power=0.05, precision=precision)
+    with Lattice(mask, **kw) as lat:
+        lat.step(17)
+        us = lat.pattern_copy_us(launches=20)
+        assert 0.0 < us < 1e5 and lat.steps_done == 0
+        lat.step(25)
+        got = [t.cpu().numpy() for t in lat.fields()]
+    with Lattice(mask, **kw) as ref:
+        ref.step(25)
+        want = [t.cpu().numpy() for t in ref.fields()]
+    for a, b in zip(got, want):
+        assert np.array_equal(a, b)

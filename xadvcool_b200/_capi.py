@@ -103,6 +103,7 @@ SIGNATURES = {
     "xac_thermal_macroscopic": [_vp, _vp, _i, _i, _i, _vp],
     "xac_test_dirichlet_plane": [_vp, _f, _i, _i, _i, _i, _vp],
     "xac_test_bounded_waits": [C.c_uint, _vp, _vp],
+    "xac_test_set_step_status": [_vp, C.c_uint, _vp],
     "xac_test_conv_wait_timeout": [C.c_uint, _vp],
     "xac_test_periodic_stream": [_vp, _vp, _i, _i, _i, _vp],
     "xac_test_forced_bgk": [_vp, _vp, _vp, _vp, _f, _f, _i, _i, _i, _vp],
@@ -118,6 +119,7 @@ SIGNATURES = {
     "xac_lattice_get_inlet": [_vp, C.POINTER(_d), _vp],
     "xac_lattice_steps_done": [_vp, C.POINTER(C.c_longlong)],
     "xac_lattice_tune": [_vp, _i, _i],
+    "xac_lattice_pattern_copy": [_vp, _i, C.POINTER(_d), _vp],
     "xac_lattice_get_tune": [_vp, C.POINTER(_i), C.POINTER(_i)],
     "xac_lattice_scalars": [_vp, C.POINTER(ScalarParams), _vp, _vp],
     "xac_scalars_fields": [_vp, _vp, _vp, _vp, _i, _i, _i, C.POINTER(ScalarParams), _vp, _vp],
@@ -138,6 +140,13 @@ SIGNATURES = {
     "xac_batch_tune": [_vp, _i, _i],
     "xac_batch_get_tune": [_vp, C.POINTER(_i), C.POINTER(_i)],
     "xac_batch_run": [_vp, C.POINTER(RunOpts), C.POINTER(RunResult), _vp],
+    "xac_batch_launch_counts": [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
+    "xac_batch_open": [_i, C.POINTER(_vp)],
+    "xac_batch_admit": [_vp, C.POINTER(Desc), C.POINTER(_i), _vp],
+    "xac_batch_advance": [_vp, C.POINTER(RunOpts), C.c_longlong, C.POINTER(_i), C.POINTER(_i), C.POINTER(RunResult),
+                          C.POINTER(_d), _vp],
+    "xac_batch_release": [_vp, _i],
+    "xac_lattice_footprint": [C.POINTER(Desc), C.POINTER(C.c_ulonglong)],
 }
 
 _lib = None

@@ -9,6 +9,11 @@
 // blocks. The per-tile reduction is the single-lattice one, so a design solved in a batch takes exactly the
 // steps and ends with exactly the bits of the same design solved alone.
 //
+// Designs may join a running batch (xac_batch_admit): each keeps the global step at which it started, always a
+// multiple of stats_every, and everything that depends on a design's own step count (its first step, its buffer
+// parity, its step limit, the convergence rule's minimum and the pump's start) is taken relative to that start.
+// Designs of xac_batch_run all start at step 0.
+//
 // The barrier waits are bounded: a wait that exceeds the spin limit records XAC_ETIMEOUT in the control block
 // and every block leaves the kernel.
 #pragma once
@@ -30,6 +35,7 @@ struct BatchDesign {
   float *rho, *ux, *uy, *uz, *T;
   uint32_t ncell, tiles, stat_tiles, row_base;
   long long min_steps;
+  long long start;  // global step at which the design joined the batch (a multiple of stats_every)
   // run state, owned by the device during a run
   int active, converged, diverged, pad;
   long long steps;
@@ -145,11 +151,8 @@ __global__ void __launch_bounds__(256, XAC_BATCH_MIN_BLOCKS) batch_persistent_ke
     // control-block fields change during the launch (retirement): read them through L2
     const int na = *(volatile int*)&ctl->n_active;
     const uint32_t total = __ldcg(ctl->prefix + na);
-    const bool own = step == 0;
     const long long s1 = step + 1;
-    const bool stats = (s1 % run.stats_every) == 0;
-    const bool macro = stats || s1 == run.max_steps;
-    const int cur = (int)(step & 1);
+    const bool stats = (s1 % run.stats_every) == 0;  // designs start on stats boundaries: the same for each
     // ---- one coupled step of every active design
     // The tile prefix of the active designs goes to shared memory once per step. A block's tiles t rise, so
     // their design slot k only moves forward: the search starts from the last slot, and the design's
@@ -169,6 +172,10 @@ __global__ void __launch_bounds__(256, XAC_BATCH_MIN_BLOCKS) batch_persistent_ke
       }
       const uint32_t tile = t - s_prefix[k];
       const BatchDesign& d = dsh;
+      const long long ls = step - d.start;  // the design's own step count
+      const bool own = ls == 0;
+      const bool macro = stats || ls + 1 == run.max_steps;
+      const int cur = (int)(ls & 1);
       if (own) {
         if (macro) batch_step_tile<S, true, true>(d, tile, cur);
         else batch_step_tile<S, false, true>(d, tile, cur);
@@ -186,7 +193,7 @@ __global__ void __launch_bounds__(256, XAC_BATCH_MIN_BLOCKS) batch_persistent_ke
         const int k = find_slot(ctl->stat_prefix, na, t);
         const BatchDesign& d = D[__ldcg(ctl->active + k)];  // geometry and pointers never change
         const uint32_t tile = t - __ldcg(ctl->stat_prefix + k);
-        const S* Qnew = (const S*)d.Q[cur ^ 1];
+        const S* Qnew = (const S*)d.Q[((step - d.start) & 1) ^ 1];
         for (uint32_t c = tile * kStatsTile + threadIdx.x; c < (tile + 1) * kStatsTile && c < d.ncell;
              c += blockDim.x)
           d.T[c] = finalize_T_cell<S, true>(Qnew, d.link, d.p, c);
@@ -226,7 +233,8 @@ __global__ void __launch_bounds__(256, XAC_BATCH_MIN_BLOCKS) batch_persistent_ke
         if (threadIdx.x == 0) {
           const double ke = st[XAC_ST_SUM_KE], max_T = st[XAC_ST_MAX_T], Q_out = st[XAC_ST_Q_OUT],
                        max_v = st[XAC_ST_MAX_V];
-          const bool past = s1 > run.stats_every;
+          const long long s1d = s1 - d.start;  // the design's own step count after this step
+          const bool past = s1d > run.stats_every;
           // the previous check of this design may have run on another block: read through L2
           const double pke = __ldcg(&d.prev_ke), pT = __ldcg(&d.prev_max_T), pQ = __ldcg(&d.prev_Q);
           d.d_ke = past ? fabs(ke - pke) / (pke + 1e-9) / run.stats_every : 0.0;
@@ -235,7 +243,7 @@ __global__ void __launch_bounds__(256, XAC_BATCH_MIN_BLOCKS) batch_persistent_ke
           d.prev_ke = ke;
           d.prev_max_T = max_T;
           d.prev_Q = Q_out;
-          if (run.constant_power && s1 > 2000) {
+          if (run.constant_power && s1d > 2000) {
             // src/simulation.py:139-146, the controller of xac_lattice_run on this design's stats
             double ue = (double)__ldcg(d.u_in);
             const double rin = st[XAC_ST_C_IN] > 0 ? st[XAC_ST_SUM_RHO_IN] / st[XAC_ST_C_IN] : 1.0;
@@ -247,8 +255,8 @@ __global__ void __launch_bounds__(256, XAC_BATCH_MIN_BLOCKS) batch_persistent_ke
             __stcg(d.u_in, (float)ue);
           }
           for (int j = 0; j < kNStats; ++j) d.last[j] = st[j];
-          d.steps = s1;
-          if (s1 > d.min_steps && d.d_ke < run.tol_ke && d.dT < run.tol_T && d.dQ < run.tol_T) {
+          d.steps = s1d;
+          if (s1d > d.min_steps && d.d_ke < run.tol_ke && d.dT < run.tol_T && d.dQ < run.tol_T) {
             d.converged = 1;
             d.active = 0;
           } else if (st[XAC_ST_NONFINITE] > 0 || max_v > 0.17 || max_T > 1e4) {

@@ -1,9 +1,11 @@
 // Lattice object of libxac.so: owns the fused-step state of one design and implements the
 // xac_lattice_* entry points (the path of src/simulation.py:14-162).
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <mutex>
 #include <utility>
 #include <vector>
@@ -139,6 +141,73 @@ __global__ void export_fields_kernel(const float* __restrict__ rho, const float*
 
 __global__ void set_scalar_kernel(float* dst, float v) { *dst = v; }
 
+// Memory-pattern probe of the fused step: the threads, the link-word reads, the population addresses (fluid pulls
+// with the bounce-back reads its link bits select, thermal pulls from the neighbours) and the whole-sector fills
+// of solid and padding lanes that coupled_step_kernel has, with no arithmetic: every value read is stored
+// unchanged at the cell's own position of the other buffer. Its time is the floor the step's memory access
+// pattern sets. (At the domain faces the thermal rules read the cell's own row instead of a neighbour: the probe
+// pulls there too, which reads padding or guard values.)
+template <typename S, int kT>
+__global__ void __launch_bounds__(256) pattern_copy_kernel(const S* __restrict__ Pin, S* __restrict__ Pout,
+                                                           const S* __restrict__ Qin, S* __restrict__ Qout,
+                                                           const uint32_t* __restrict__ link, Geom g,
+                                                           uint32_t reverse) {
+  const int RL = row_len<kT>(g);
+  const uint32_t blk = reverse ? gridDim.x - 1u - blockIdx.x : blockIdx.x;
+  const uint32_t pos = blk * blockDim.x + threadIdx.x;
+  const uint32_t r = pos / (uint32_t)RL, x = pos - r * (uint32_t)RL;
+  if (r >= (uint32_t)g.rows) return;  // whole warps (the row length is a multiple of 32)
+  const int lane = threadIdx.x & 31;
+  const bool valid = x < (uint32_t)g.nx;
+  const uint32_t c = r * (uint32_t)g.nx + x;
+  const uint32_t lw = valid ? __ldg(link + c) : ((uint32_t)kSolid << kTypeShift);
+  const bool fluid = valid && link_type(lw) != kSolid;
+  const unsigned grp = sector_group<S>(lane);
+  const bool fill_p = (__ballot_sync(0xffffffffu, fluid) & grp) != 0u;
+  const bool fill_q = (__ballot_sync(0xffffffffu, valid) & grp) != 0u;
+  const uint32_t e0 = pop_base(r, x, g, RL);
+  const S zero = static_cast<S>(0.0f);
+  if (fluid) {
+    const Rows<S, kT> P = rows_at<kT>(Pin, e0, g, RL);
+#define XAC_PC_P(I) Pout[e0 + (I) * RL] = ((lw >> (I)) & 1u) ? __ldg(P.own(opp_of(I))) : __ldg(P.template pull<I>());
+    XAC_FOR19(XAC_PC_P)
+#undef XAC_PC_P
+  } else if (fill_p) {
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) Pout[e0 + i * RL] = zero;
+  }
+  if (valid) {
+    const Rows<S, kT> Q = rows_at<kT>(Qin, e0, g, RL);
+#define XAC_PC_Q(I) Qout[e0 + (I) * RL] = __ldg(Q.template pull<I>());
+    XAC_FOR19(XAC_PC_Q)
+#undef XAC_PC_Q
+  } else if (fill_q) {
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) Qout[e0 + i * RL] = zero;
+  }
+}
+
+template <typename S>
+void launch_pattern_copy(const void* Pin, void* Pout, const void* Qin, void* Qout, const uint32_t* link, const Geom& g,
+                         int block, uint32_t reverse, cudaStream_t s) {
+  const unsigned grid = (unsigned)(((long long)g.rows * g.pitch + block - 1) / block);
+#define XAC_PC(KT)                                                                                                 \
+  pattern_copy_kernel<S, KT><<<grid, block, 0, s>>>((const S*)Pin, (S*)Pout, (const S*)Qin, (S*)Qout, link, g, \
+                                                    reverse)
+  switch (g.pitch) {
+    case 32: XAC_PC(32); break;
+    case 64: XAC_PC(64); break;
+    case 96: XAC_PC(96); break;
+    case 128: XAC_PC(128); break;
+    case 160: XAC_PC(160); break;
+    case 192: XAC_PC(192); break;
+    case 224: XAC_PC(224); break;
+    case 256: XAC_PC(256); break;
+    default: XAC_PC(0);
+  }
+#undef XAC_PC
+}
+
 template <typename T>
 int dmalloc(T** p, size_t count, const char* what) {
   cudaError_t e = cudaMalloc((void**)p, count * sizeof(T) + 16);
@@ -230,6 +299,14 @@ struct LatticeImpl {
   int tune_block = 128;  // threads per block of the step kernel
   int tune_variant = 0;  // 0: one thread per row position; 1: thermal rows staged in shared memory
   unsigned* status = nullptr;  // device word set by a step kernel whose bounded wait ran out
+  // set once the status word was seen non-zero: a staged step gave up on its copies, so the thermal populations it
+  // wrote are not the step's; the lattice refuses work until init_fields / load_state rewrites its populations
+  bool failed = false;
+  int refuse(const char* fn) const {
+    set_error("%s: this lattice stopped being usable when a staged step kernel gave up waiting for its copies; "
+              "re-initialise it (init_fields) or load a saved state", fn);
+    return XAC_ETIMEOUT;
+  }
 
   void* P[2] = {nullptr, nullptr};
   void* Qb[2] = {nullptr, nullptr};
@@ -761,13 +838,26 @@ int xac_lattice_destroy(xac_lattice* lat) {
 int xac_lattice_init_fields(xac_lattice* lat, const float* rho, const float* u, const float* T, void* stream) {
   XAC_REQUIRE(lat, "xac_lattice_init_fields: null lattice");
   std::lock_guard<std::mutex> g(lat->impl.mu);
-  return init_impl(lat->impl, rho, u, T, as_stream(stream));
+  LatticeImpl& L = lat->impl;
+  XAC_CUDA(cudaMemsetAsync(L.status, 0, sizeof(unsigned), as_stream(stream)));
+  L.failed = false;
+  return init_impl(L, rho, u, T, as_stream(stream));
+}
+
+int xac_test_set_step_status(xac_lattice* lat, unsigned value, void* stream) {
+  XAC_REQUIRE(lat, "xac_test_set_step_status: null lattice");
+  std::lock_guard<std::mutex> g(lat->impl.mu);
+  cudaStream_t s = as_stream(stream);
+  XAC_CUDA(cudaMemcpyAsync(lat->impl.status, &value, sizeof(value), cudaMemcpyHostToDevice, s));
+  XAC_CUDA(cudaStreamSynchronize(s));
+  return XAC_OK;
 }
 
 int xac_lattice_step(xac_lattice* lat, int n, void* stream) {
   XAC_REQUIRE(lat, "xac_lattice_step: null lattice");
   XAC_REQUIRE(n >= 0, "xac_lattice_step: negative step count %d", n);
   std::lock_guard<std::mutex> g(lat->impl.mu);
+  if (lat->impl.failed) return lat->impl.refuse("xac_lattice_step");
   return lat->impl.steps(n, as_stream(stream));
 }
 
@@ -775,6 +865,7 @@ int xac_lattice_stats(xac_lattice* lat, double* out_host, void* stream) {
   XAC_REQUIRE(lat && out_host, "xac_lattice_stats: null pointer");
   LatticeImpl& L = lat->impl;
   std::lock_guard<std::mutex> g(L.mu);
+  if (L.failed) return L.refuse("xac_lattice_stats");
   cudaStream_t s = as_stream(stream);
   int r = L.finalize_T(s);
   if (r != XAC_OK) return r;
@@ -786,7 +877,9 @@ int xac_lattice_stats(xac_lattice* lat, double* out_host, void* stream) {
     XAC_CUDA(cudaMemcpyAsync(&st, L.status, sizeof(st), cudaMemcpyDeviceToHost, s));
     XAC_CUDA(cudaStreamSynchronize(s));
     if (st) {
-      set_error("xac_lattice_stats: a staged step kernel gave up waiting for its copies (status %u)", st);
+      L.failed = true;
+      set_error("xac_lattice_stats: a staged step kernel gave up waiting for its copies (status %u); the lattice "
+                "refuses further work until init_fields or load_state", st);
       return XAC_ETIMEOUT;
     }
   }
@@ -797,6 +890,7 @@ int xac_lattice_fields(xac_lattice* lat, float* rho, float* u, float* T, void* s
   XAC_REQUIRE(lat, "xac_lattice_fields: null lattice");
   LatticeImpl& L = lat->impl;
   std::lock_guard<std::mutex> g(L.mu);
+  if (L.failed) return L.refuse("xac_lattice_fields");
   cudaStream_t s = as_stream(stream);
   if (T) {
     int r = L.finalize_T(s);
@@ -820,6 +914,45 @@ int xac_lattice_get_inlet(xac_lattice* lat, double* u_inlet, void*) {
   XAC_REQUIRE(lat && u_inlet, "xac_lattice_get_inlet: null pointer");
   *u_inlet = (double)lat->impl.u_in_host;
   return XAC_OK;
+}
+
+int xac_lattice_pattern_copy(xac_lattice* lat, int launches, double* us_per_launch, void* stream) {
+  XAC_REQUIRE(lat && us_per_launch, "xac_lattice_pattern_copy: null pointer");
+  XAC_REQUIRE(launches >= 1 && launches <= 100000, "xac_lattice_pattern_copy: launches %d out of 1..100000",
+              launches);
+  LatticeImpl& L = lat->impl;
+  std::lock_guard<std::mutex> g(L.mu);
+  cudaStream_t s = as_stream(stream);
+  auto launch = [&](int k) {
+    const int c = k & 1;
+    switch (L.precision) {
+      case XAC_FP16:
+        launch_pattern_copy<__half>(L.P[c], L.P[c ^ 1], L.Qb[c], L.Qb[c ^ 1], L.link, L.g, L.tune_block, c, s);
+        break;
+      case XAC_BF16:
+        launch_pattern_copy<__nv_bfloat16>(L.P[c], L.P[c ^ 1], L.Qb[c], L.Qb[c ^ 1], L.link, L.g, L.tune_block, c, s);
+        break;
+      default:
+        launch_pattern_copy<float>(L.P[c], L.P[c ^ 1], L.Qb[c], L.Qb[c ^ 1], L.link, L.g, L.tune_block, c, s);
+    }
+  };
+  for (int k = 0; k < 4; ++k) launch(k);  // warm-up
+  cudaEvent_t a = nullptr, b = nullptr;
+  XAC_CUDA(cudaEventCreate(&a));
+  cudaError_t e = cudaEventCreate(&b);
+  if (e == cudaSuccess) e = cudaEventRecord(a, s);
+  for (int k = 0; e == cudaSuccess && k < launches; ++k) launch(k);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaEventRecord(b, s);
+  if (e == cudaSuccess) e = cudaEventSynchronize(b);
+  float ms = 0.0f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  if (e != cudaSuccess) return cuda_status(e, "xac_lattice_pattern_copy");
+  *us_per_launch = (double)ms * 1e3 / launches;
+  // the probe left copies, not a physical state: start the lattice over from the cold start
+  return init_impl(L, nullptr, nullptr, nullptr, s);
 }
 
 int xac_lattice_tune(xac_lattice* lat, int block, int variant) {
@@ -858,6 +991,7 @@ int xac_lattice_scalars(xac_lattice* lat, const xac_scalar_params* prm, double* 
   LatticeImpl& L = lat->impl;
   XAC_REQUIRE(prm->buf >= 0 && 2 * prm->buf < L.g.nx, "xac_lattice_scalars: bad buffer length %d", prm->buf);
   std::lock_guard<std::mutex> g(L.mu);
+  if (L.failed) return L.refuse("xac_lattice_scalars");
   cudaStream_t s = as_stream(stream);
   int r = L.finalize_T(s);
   if (r != XAC_OK) return r;
@@ -873,6 +1007,7 @@ int xac_lattice_validate(xac_lattice* lat, double* out_host, void* stream) {
   XAC_REQUIRE(lat && out_host, "xac_lattice_validate: null pointer");
   LatticeImpl& L = lat->impl;
   std::lock_guard<std::mutex> g(L.mu);
+  if (L.failed) return L.refuse("xac_lattice_validate");
   cudaStream_t s = as_stream(stream);
   int r = L.finalize_T(s);  // rho and u are written by the last step of every step call
   if (r != XAC_OK) return r;
@@ -904,6 +1039,7 @@ int xac_lattice_save_state(xac_lattice* lat, void* host_dst, size_t bytes, void*
   XAC_REQUIRE(bytes >= need, "xac_lattice_save_state: buffer of %zu bytes, need %zu", bytes, need);
   LatticeImpl& L = lat->impl;
   std::lock_guard<std::mutex> g(L.mu);
+  if (L.failed) return L.refuse("xac_lattice_save_state");
   cudaStream_t s = as_stream(stream);
   int r = L.finalize_T(s);
   if (r != XAC_OK) return r;
@@ -950,7 +1086,9 @@ int xac_lattice_load_state(xac_lattice* lat, const void* host_src, size_t bytes,
   std::memcpy(&u_in, &hdr[7], sizeof(float));
   L.u_in_host = u_in;
   set_scalar_kernel<<<1, 1, 0, s>>>(L.u_in, u_in);
+  XAC_CUDA(cudaMemsetAsync(L.status, 0, sizeof(unsigned), s));
   XAC_CUDA(cudaStreamSynchronize(s));
+  L.failed = false;
   L.cur = 0;
   L.step = hdr[5];
   L.own_pending = hdr[6] != 0;
@@ -1017,6 +1155,7 @@ int xac_lattice_run(xac_lattice* lat, const xac_run_opts* o, xac_run_result* res
   XAC_REQUIRE(lat && o && res, "xac_lattice_run: null pointer");
   XAC_REQUIRE(o->stats_every > 0 && o->max_steps >= 0, "xac_lattice_run: bad options");
   LatticeImpl& L = lat->impl;
+  if (L.failed) return L.refuse("xac_lattice_run");
   std::memset(res, 0, sizeof(*res));
   const long long min_steps = o->min_steps > 0 ? o->min_steps : L.reference_min_steps(o->max_steps);
   double prev_ke = 0.0, prev_max_T = 0.0, d_ke = 0.0, dT = 0.0, prev_Q = 0.0, dQ = 1.0;
@@ -1109,7 +1248,9 @@ int xac_lattice_run(xac_lattice* lat, const xac_run_opts* o, xac_run_result* res
         unsigned stw = 0;
         XAC_CUDA(cudaMemcpy(&stw, L.status, sizeof(stw), cudaMemcpyDeviceToHost));
         if (stw) {
-          set_error("xac_lattice_run: a staged step kernel gave up waiting for its copies (status %u)", stw);
+          L.failed = true;
+          set_error("xac_lattice_run: a staged step kernel gave up waiting for its copies (status %u); the lattice "
+                    "refuses further work until init_fields or load_state", stw);
           return XAC_ETIMEOUT;
         }
       }
@@ -1215,7 +1356,14 @@ int xac_scalars_fields(const float* rho, const float* u, const float* T, const i
 // Batch of designs advanced by one persistent cooperative launch (batch.cuh)
 // =====================================================================================================
 struct xac_batch {
-  std::vector<xac_lattice*> lats;
+  std::vector<xac_lattice*> lats;  // slot -> design (open batches: nullptr for a free slot)
+  // open batches (xac_batch_open): designs join and leave while the batch runs
+  enum : int { kFree = 0, kPending = 1, kActive = 2, kDone = 3 };
+  bool open = false;
+  std::vector<int> state;      // per slot
+  std::vector<double> gpu_s;   // per slot: its share of the launches' wall time since it joined
+  long long gstep = 0;         // global step of the batch
+  long long graph_launches = 0, direct_launches = 0;
   int precision = XAC_FP32;
   int block = 128;              // threads per block (= cells per tile)
   int steps_per_launch = 1000;  // steps one launch may advance
@@ -1225,10 +1373,18 @@ struct xac_batch {
   size_t rows_cap = 0;
   BatchCtl* hC = nullptr;  // pinned
   std::vector<BatchDesign> hD;
-  std::map<std::pair<int, long long>, cudaGraphExec_t> graphs;
+  // captured persistent launches, keyed by every launch option they hold; the device pointers they hold (designs,
+  // control block, stats rows) are the batch's for its lifetime, except the stats rows of an open batch, whose
+  // reallocation drops every cached graph
+  std::map<std::tuple<int, long long, int, double, double, int, double>, cudaGraphExec_t> graphs;
+  void drop_graphs() {
+    for (auto& kv : graphs)
+      if (kv.second) cudaGraphExecDestroy(kv.second);
+    graphs.clear();
+  }
   cudaStream_t capture = nullptr;
   ~xac_batch() {
-    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    drop_graphs();
     if (capture) cudaStreamDestroy(capture);
     cudaFree(dD);
     cudaFree(dC);
@@ -1263,7 +1419,9 @@ int batch_launch(xac_batch* b, const BatchRun& run, cudaStream_t s, bool use_gra
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   if (use_graph) {
-    auto key = std::make_pair(run.steps, run.max_steps);
+    const auto key =
+        std::make_tuple(run.steps, run.max_steps, run.stats_every, run.tol_ke, run.tol_T, run.constant_power,
+                        run.target_power);
     auto it = b->graphs.find(key);
     if (it == b->graphs.end()) {
       if (!b->capture) XAC_CUDA(cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking));
@@ -1286,12 +1444,90 @@ int batch_launch(xac_batch* b, const BatchRun& run, cudaStream_t s, bool use_gra
     }
     if (it->second) {
       XAC_CUDA(cudaGraphLaunch(it->second, s));
+      ++b->graph_launches;
       return XAC_OK;
     }
   }
   cfg.stream = s;
   XAC_CUDA(cudaLaunchKernelExC(&cfg, (const void*)batch_persistent_kernel<S>, args));
+  ++b->direct_launches;
   return XAC_OK;
+}
+
+int batch_launch_any(xac_batch* b, const BatchRun& run, cudaStream_t s, bool use_graph) {
+  switch (b->precision) {
+    case XAC_FP16: return batch_launch<__half>(b, run, s, use_graph);
+    case XAC_BF16: return batch_launch<__nv_bfloat16>(b, run, s, use_graph);
+    default: return batch_launch<float>(b, run, s, use_graph);
+  }
+}
+
+// Descriptor of design L for the persistent kernel, joining the batch at global step `start`.
+void fill_design(BatchDesign& d, LatticeImpl& L, int block, long long min_steps, long long start) {
+  d = BatchDesign{};
+  d.p = L.params();
+  d.P[0] = L.P[0];
+  d.P[1] = L.P[1];
+  d.Q[0] = L.Qb[0];
+  d.Q[1] = L.Qb[1];
+  d.link = L.link;
+  d.qsrc = L.qsrc;
+  d.u_in = L.u_in;
+  d.rho = L.rho;
+  d.ux = L.ux;
+  d.uy = L.uy;
+  d.uz = L.uz;
+  d.T = L.T;
+  d.ncell = (uint32_t)L.g.ncell;
+  d.tiles = (uint32_t)(((long long)L.g.rows * L.g.pitch + block - 1) / block);  // row positions
+  d.stat_tiles = (uint32_t)stats_tiles(L.g.ncell);
+  d.min_steps = min_steps;
+  d.start = start;
+  d.active = 1;
+  d.dQ = 1.0;
+}
+
+// Control block of a launch over the designs in `act` (slot indices, ascending): active list, tile prefixes and
+// the stats rows of each design (packed in list order).
+void build_ctl(xac_batch* b, const std::vector<int>& act, long long step) {
+  std::memset(b->hC, 0, sizeof(BatchCtl));
+  uint32_t acc = 0, sacc = 0;
+  for (size_t k = 0; k < act.size(); ++k) {
+    BatchDesign& d = b->hD[act[k]];
+    d.row_base = sacc;
+    b->hC->active[k] = (uint32_t)act[k];
+    b->hC->prefix[k] = acc;
+    b->hC->stat_prefix[k] = sacc;
+    acc += d.tiles;
+    sacc += d.stat_tiles;
+  }
+  b->hC->prefix[act.size()] = acc;
+  b->hC->stat_prefix[act.size()] = sacc;
+  b->hC->n_active = (int)act.size();
+  b->hC->all_done = act.empty() ? 1 : 0;
+  b->hC->step = step;
+}
+
+// A finished design's outcome, and its lattice left at its last step (fields, stats and scalars then read it).
+void finish_design(xac_batch* b, int slot, long long steps, float u_fin, const xac_run_opts* o, xac_run_result& rr) {
+  const BatchDesign& d = b->hD[slot];
+  std::memset(&rr, 0, sizeof(rr));
+  rr.steps = steps;
+  rr.diverged = d.diverged;
+  rr.converged = d.converged ? 1 : (!d.diverged && steps > d.min_steps && d.d_ke < o->tol_ke && d.dT < o->tol_T &&
+                                    d.dQ < o->tol_T);
+  rr.d_ke = d.d_ke;
+  rr.dT_conv = d.dT;
+  rr.dQ_conv = d.dQ;
+  rr.u_inlet_final = (double)u_fin;
+  std::memcpy(rr.last_stats, d.last, sizeof(d.last));
+  LatticeImpl& L = b->lats[slot]->impl;
+  L.u_in_host = u_fin;
+  L.step = steps;
+  L.cur = (int)(steps & 1);
+  L.own_pending = steps == 0;
+  L.macro_step = steps;
+  L.T_step = (steps % o->stats_every == 0) ? steps : -1;
 }
 
 }  // namespace
@@ -1354,6 +1590,7 @@ int xac_batch_size(const xac_batch* b, int* n) {
 int xac_batch_lattice(xac_batch* b, int i, xac_lattice** lat) {
   XAC_REQUIRE(b && lat, "xac_batch_lattice: null pointer");
   XAC_REQUIRE(i >= 0 && i < (int)b->lats.size(), "xac_batch_lattice: index %d out of range", i);
+  XAC_REQUIRE(b->lats[i], "xac_batch_lattice: slot %d holds no design", i);
   *lat = b->lats[i];
   return XAC_OK;
 }
@@ -1363,9 +1600,7 @@ int xac_batch_tune(xac_batch* b, int block, int steps_per_launch) {
   XAC_REQUIRE(block == 64 || block == 128 || block == 256, "xac_batch_tune: block must be 64, 128 or 256");
   XAC_REQUIRE(steps_per_launch >= 1, "xac_batch_tune: steps_per_launch must be positive");
   if (b->block != block) {
-    for (auto& kv : b->graphs)
-      if (kv.second) cudaGraphExecDestroy(kv.second);
-    b->graphs.clear();
+    b->drop_graphs();
   }
   b->block = block;
   b->steps_per_launch = steps_per_launch;
@@ -1381,51 +1616,20 @@ int xac_batch_get_tune(const xac_batch* b, int* block, int* steps_per_launch) {
 
 int xac_batch_run(xac_batch* b, const xac_run_opts* o, xac_run_result* res, void* stream) {
   XAC_REQUIRE(b && o && res, "xac_batch_run: null pointer");
+  XAC_REQUIRE(!b->open, "xac_batch_run: an open batch advances with xac_batch_advance");
   XAC_REQUIRE(o->stats_every > 0 && o->max_steps >= 0, "xac_batch_run: bad options");
   cudaStream_t s = as_stream(stream);
   const int n = (int)b->lats.size();
   b->hD.assign(n, BatchDesign{});
-  uint32_t row = 0;
+  std::vector<int> act(n);
   for (int i = 0; i < n; ++i) {
     LatticeImpl& L = b->lats[i]->impl;
     XAC_REQUIRE(L.step == 0 && L.own_pending,
                 "xac_batch_run: design %d is not at step 0 (create it or re-initialise it with init_fields)", i);
-    BatchDesign& d = b->hD[i];
-    d.p = L.params();
-    d.P[0] = L.P[0];
-    d.P[1] = L.P[1];
-    d.Q[0] = L.Qb[0];
-    d.Q[1] = L.Qb[1];
-    d.link = L.link;
-    d.qsrc = L.qsrc;
-    d.u_in = L.u_in;
-    d.rho = L.rho;
-    d.ux = L.ux;
-    d.uy = L.uy;
-    d.uz = L.uz;
-    d.T = L.T;
-    d.ncell = (uint32_t)L.g.ncell;
-    d.tiles = (uint32_t)(((long long)L.g.rows * L.g.pitch + b->block - 1) / b->block);  // row positions
-    d.stat_tiles = (uint32_t)stats_tiles(L.g.ncell);
-    d.row_base = row;
-    row += d.stat_tiles;
-    d.min_steps = o->min_steps > 0 ? o->min_steps : L.reference_min_steps(o->max_steps);
-    d.active = 1;
-    d.dQ = 1.0;
+    fill_design(b->hD[i], L, b->block, o->min_steps > 0 ? o->min_steps : L.reference_min_steps(o->max_steps), 0);
+    act[i] = i;
   }
-  std::memset(b->hC, 0, sizeof(BatchCtl));
-  uint32_t acc = 0, sacc = 0;
-  for (int i = 0; i < n; ++i) {
-    b->hC->active[i] = (uint32_t)i;
-    b->hC->prefix[i] = acc;
-    b->hC->stat_prefix[i] = sacc;
-    acc += b->hD[i].tiles;
-    sacc += b->hD[i].stat_tiles;
-  }
-  b->hC->prefix[n] = acc;
-  b->hC->stat_prefix[n] = sacc;
-  b->hC->n_active = n;
-  b->hC->all_done = n == 0 ? 1 : 0;
+  build_ctl(b, act, 0);
   XAC_CUDA(cudaMemcpyAsync(b->dD, b->hD.data(), n * sizeof(BatchDesign), cudaMemcpyHostToDevice, s));
   XAC_CUDA(cudaMemcpyAsync(b->dC, b->hC, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
   BatchRun run{};
@@ -1440,12 +1644,7 @@ int xac_batch_run(xac_batch* b, const xac_run_opts* o, xac_run_result* res, void
   while (done < o->max_steps && !b->hC->all_done) {
     const long long left = o->max_steps - done;
     run.steps = (int)(left < b->steps_per_launch ? left : b->steps_per_launch);
-    int r;
-    switch (b->precision) {
-      case XAC_FP16: r = batch_launch<__half>(b, run, s, true); break;
-      case XAC_BF16: r = batch_launch<__nv_bfloat16>(b, run, s, true); break;
-      default: r = batch_launch<float>(b, run, s, true);
-    }
+    int r = batch_launch_any(b, run, s, true);
     if (r != XAC_OK) return r;
     XAC_CUDA(cudaMemcpyAsync(b->hC, b->dC, 32, cudaMemcpyDeviceToHost, s));  // barrier words, err, done, step
     XAC_CUDA(cudaStreamSynchronize(s));
@@ -1460,28 +1659,190 @@ int xac_batch_run(xac_batch* b, const xac_run_opts* o, xac_run_result* res, void
   for (int i = 0; i < n; ++i)  // the inlet velocities the pump left (one small copy per design)
     XAC_CUDA(cudaMemcpyAsync(&u_fin[i], b->lats[i]->impl.u_in, sizeof(float), cudaMemcpyDeviceToHost, s));
   XAC_CUDA(cudaStreamSynchronize(s));
-  for (int i = 0; i < n; ++i) {
-    const BatchDesign& d = b->hD[i];
-    xac_run_result& rr = res[i];
-    std::memset(&rr, 0, sizeof(rr));
-    const long long steps = d.active ? done : d.steps;
-    rr.steps = steps;
-    rr.diverged = d.diverged;
-    rr.converged = d.converged ? 1 : (!d.diverged && steps > d.min_steps && d.d_ke < o->tol_ke && d.dT < o->tol_T &&
-                                      d.dQ < o->tol_T);
-    rr.d_ke = d.d_ke;
-    rr.dT_conv = d.dT;
-    rr.dQ_conv = d.dQ;
-    LatticeImpl& L = b->lats[i]->impl;
-    L.u_in_host = u_fin[i];
-    rr.u_inlet_final = (double)u_fin[i];
-    std::memcpy(rr.last_stats, d.last, sizeof(d.last));
-    L.step = steps;
-    L.cur = (int)(steps & 1);
-    L.own_pending = steps == 0;
-    L.macro_step = steps;
-    L.T_step = (steps % o->stats_every == 0) ? steps : -1;
+  for (int i = 0; i < n; ++i) finish_design(b, i, b->hD[i].active ? done : b->hD[i].steps, u_fin[i], o, res[i]);
+  return XAC_OK;
+}
+
+int xac_batch_launch_counts(const xac_batch* b, long long* graph_launches, long long* direct_launches) {
+  XAC_REQUIRE(b && graph_launches && direct_launches, "xac_batch_launch_counts: null pointer");
+  *graph_launches = b->graph_launches;
+  *direct_launches = b->direct_launches;
+  return XAC_OK;
+}
+
+int xac_batch_open(int precision, xac_batch** out) {
+  XAC_REQUIRE(out, "xac_batch_open: null pointer");
+  XAC_REQUIRE(precision == XAC_FP32 || precision == XAC_FP16 || precision == XAC_BF16,
+              "xac_batch_open: unknown precision %d", precision);
+  *out = nullptr;
+  xac_batch* b = new (std::nothrow) xac_batch();
+  if (!b) {
+    set_error("xac_batch_open: host allocation failed");
+    return XAC_ENOMEM;
   }
+  b->open = true;
+  b->precision = precision;
+  b->hD.assign(kMaxBatch, BatchDesign{});
+  int r = XAC_OK;
+  if ((r = dmalloc(&b->dD, (size_t)kMaxBatch, "alloc batch designs")) != XAC_OK ||
+      (r = dmalloc(&b->dC, 1, "alloc batch control")) != XAC_OK) {
+    delete b;
+    return r;
+  }
+  if (cudaMallocHost(&b->hC, sizeof(BatchCtl)) != cudaSuccess) {
+    delete b;
+    set_error("xac_batch_open: pinned allocation failed");
+    return XAC_ENOMEM;
+  }
+  *out = b;
+  return XAC_OK;
+}
+
+int xac_batch_admit(xac_batch* b, const xac_desc* desc, int* slot, void* stream) {
+  XAC_REQUIRE(b && desc && slot, "xac_batch_admit: null pointer");
+  XAC_REQUIRE(b->open, "xac_batch_admit: not an open batch (create it with xac_batch_open)");
+  XAC_REQUIRE(desc->precision == b->precision, "xac_batch_admit: design precision %d differs from the batch's %d",
+              desc->precision, b->precision);
+  int k = 0;
+  while (k < (int)b->lats.size() && b->state[k] != xac_batch::kFree) ++k;
+  XAC_REQUIRE(k < kMaxBatch, "xac_batch_admit: all %d slots hold designs (release finished ones first)", kMaxBatch);
+  xac_lattice* l = nullptr;
+  int r = xac_lattice_create(desc, &l, stream);
+  if (r != XAC_OK) return r;
+  if (k == (int)b->lats.size()) {
+    b->lats.push_back(nullptr);
+    b->state.push_back(xac_batch::kFree);
+    b->gpu_s.push_back(0.0);
+  }
+  b->lats[k] = l;
+  b->state[k] = xac_batch::kPending;
+  b->gpu_s[k] = 0.0;
+  *slot = k;
+  return XAC_OK;
+}
+
+int xac_batch_release(xac_batch* b, int slot) {
+  XAC_REQUIRE(b, "xac_batch_release: null batch");
+  XAC_REQUIRE(b->open, "xac_batch_release: not an open batch");
+  XAC_REQUIRE(slot >= 0 && slot < (int)b->lats.size() && b->state[slot] != xac_batch::kFree,
+              "xac_batch_release: slot %d holds no design", slot);
+  XAC_REQUIRE(b->state[slot] != xac_batch::kActive, "xac_batch_release: design %d is still running", slot);
+  xac_lattice_destroy(b->lats[slot]);
+  b->lats[slot] = nullptr;
+  b->state[slot] = xac_batch::kFree;
+  return XAC_OK;
+}
+
+int xac_batch_advance(xac_batch* b, const xac_run_opts* o, long long steps, int* n_finished, int* slots,
+                      xac_run_result* results, double* gpu_seconds, void* stream) {
+  XAC_REQUIRE(b && o && n_finished && slots && results && gpu_seconds, "xac_batch_advance: null pointer");
+  XAC_REQUIRE(b->open, "xac_batch_advance: not an open batch (create it with xac_batch_open)");
+  XAC_REQUIRE(o->stats_every > 0 && o->max_steps > 0 && steps >= 0, "xac_batch_advance: bad options");
+  cudaStream_t s = as_stream(stream);
+  *n_finished = 0;
+  BatchRun run{};
+  run.max_steps = o->max_steps;
+  run.stats_every = o->stats_every;
+  run.tol_ke = o->tol_ke;
+  run.tol_T = o->tol_T;
+  run.spin_limit = 1ull << 27;
+  run.constant_power = o->constant_power;
+  run.target_power = o->target_power;
+  const int nslots = (int)b->lats.size();
+  long long left = steps;
+  while (left > 0) {
+    // waiting designs join on a stats boundary
+    const bool boundary = b->gstep % o->stats_every == 0;
+    bool waiting = false;
+    std::vector<int> act;
+    for (int k = 0; k < nslots; ++k) {
+      if (b->state[k] == xac_batch::kPending) {
+        if (boundary) {
+          LatticeImpl& L = b->lats[k]->impl;
+          XAC_REQUIRE(L.step == 0 && L.own_pending, "xac_batch_advance: design %d is not at step 0", k);
+          fill_design(b->hD[k], L, b->block, o->min_steps > 0 ? o->min_steps : L.reference_min_steps(o->max_steps),
+                      b->gstep);
+          b->state[k] = xac_batch::kActive;
+          b->gpu_s[k] = 0.0;
+        } else {
+          waiting = true;
+        }
+      }
+      if (b->state[k] == xac_batch::kActive) act.push_back(k);
+    }
+    if (act.empty()) {
+      if (!waiting) break;
+      b->gstep += o->stats_every - b->gstep % o->stats_every;  // nothing runs until the next boundary
+      continue;
+    }
+    long long n = left < b->steps_per_launch ? left : b->steps_per_launch;
+    for (int k : act) {  // no design passes its own step limit inside a launch
+      const long long to_limit = b->hD[k].start + o->max_steps - b->gstep;
+      if (to_limit < n) n = to_limit;
+    }
+    if (waiting && o->stats_every - b->gstep % o->stats_every < n) n = o->stats_every - b->gstep % o->stats_every;
+    size_t rows = 0;
+    for (int k : act) rows += b->hD[k].stat_tiles;
+    if (rows > b->rows_cap) {
+      b->drop_graphs();  // they hold the old rows pointer
+      XAC_CUDA(cudaStreamSynchronize(s));
+      cudaFree(b->drows);
+      b->drows = nullptr;
+      b->rows_cap = 0;
+      int r = dmalloc(&b->drows, rows * kNStats + rows / 2 * kNStats, "alloc batch rows");
+      if (r != XAC_OK) return r;
+      b->rows_cap = rows + rows / 2;
+    }
+    build_ctl(b, act, b->gstep);
+    XAC_CUDA(cudaMemcpyAsync(b->dD, b->hD.data(), nslots * sizeof(BatchDesign), cudaMemcpyHostToDevice, s));
+    XAC_CUDA(cudaMemcpyAsync(b->dC, b->hC, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
+    run.steps = (int)n;
+    const auto t0 = std::chrono::steady_clock::now();
+    int r = batch_launch_any(b, run, s, n == b->steps_per_launch);
+    if (r != XAC_OK) return r;
+    XAC_CUDA(cudaMemcpyAsync(b->hC, b->dC, 32, cudaMemcpyDeviceToHost, s));
+    XAC_CUDA(cudaMemcpyAsync(b->hD.data(), b->dD, nslots * sizeof(BatchDesign), cudaMemcpyDeviceToHost, s));
+    XAC_CUDA(cudaStreamSynchronize(s));
+    const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (b->hC->err) {
+      set_error("xac_batch_advance: a grid-barrier wait gave up (device status %d)", b->hC->err);
+      return XAC_ETIMEOUT;
+    }
+    const long long ran = b->hC->step - b->gstep;
+    b->gstep = b->hC->step;
+    left -= ran;
+    // the launch's wall time, shared by the designs in proportion to their tiles
+    double tiles = 0.0;
+    for (int k : act) tiles += b->hD[k].tiles;
+    for (int k : act) b->gpu_s[k] += dt * b->hD[k].tiles / tiles;
+    for (int k : act) {
+      const BatchDesign& d = b->hD[k];
+      const long long own = b->gstep - d.start;
+      if (d.active && own < o->max_steps) continue;
+      float u_fin = 0.0f;
+      XAC_CUDA(cudaMemcpy(&u_fin, b->lats[k]->impl.u_in, sizeof(float), cudaMemcpyDeviceToHost));
+      const int m = (*n_finished)++;
+      slots[m] = k;
+      gpu_seconds[m] = b->gpu_s[k];
+      finish_design(b, k, d.active ? own : d.steps, u_fin, o, results[m]);
+      b->state[k] = xac_batch::kDone;
+    }
+    if (ran == 0 || *n_finished > 0) break;  // the caller may refill the finished designs' slots now
+  }
+  return XAC_OK;
+}
+
+// Device bytes a lattice of this descriptor allocates (populations, link words, fields, reduction rows).
+int xac_lattice_footprint(const xac_desc* d, unsigned long long* bytes) {
+  XAC_REQUIRE(d && bytes, "xac_lattice_footprint: null pointer");
+  XAC_REQUIRE(d->nx >= 1 && d->ny >= 1 && d->nz >= 1, "xac_lattice_footprint: bad lattice size");
+  const long long n = (long long)d->nx * d->ny * d->nz;
+  const long long pitch = (d->nx + 31) / 32 * 32;
+  const long long N = ((long long)d->ny * d->nz + 2LL * (d->ny + 2)) * kQ * pitch;
+  const long long elem = d->precision == XAC_FP32 ? 4 : 2;
+  const long long metric_rows = (long long)reduction_blocks(n) * kNMetrics, stat_rows = stats_tiles(n) * kNStats;
+  *bytes = (unsigned long long)(4 * N * elem + n * (1 + 4 + 4 + 5 * 4) +
+                                8 * (metric_rows > stat_rows ? metric_rows : stat_rows) + 64 * 8 + 64);
   return XAC_OK;
 }
 

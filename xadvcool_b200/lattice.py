@@ -106,6 +106,14 @@ class Lattice:
         position; 1: one block per row with the thermal input staged in shared memory). Results are unaffected."""
         _capi.call("xac_lattice_tune", self._h, int(block), int(variant))
 
+    def pattern_copy_us(self, launches: int = 200) -> float:
+        """Microseconds per launch of a kernel that moves exactly the step's populations with no arithmetic (the
+        memory-pattern floor of the step for this design); leaves the lattice at the cold start (step 0)."""
+        us = C.c_double()
+        with torch.cuda.device(self.device):
+            _capi.call("xac_lattice_pattern_copy", self._h, int(launches), C.byref(us), stream_ptr(self.device))
+        return float(us.value)
+
     def get_tune(self):
         b, v = C.c_int(), C.c_int()
         _capi.call("xac_lattice_get_tune", self._h, C.byref(b), C.byref(v))
