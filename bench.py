@@ -365,7 +365,7 @@ def forms_probe(dev, mask, lat_kw, shape):
     from xadvcool_b200.batch import Batch
     from xadvcool_b200.lattice import Lattice
     out = {}
-    for prec in ("fp16", "bf16"):
+    for prec in ("fp32_t16", "fp16", "bf16"):
         lat = Lattice(mask, device=dev, precision=prec, **lat_kw)
         lat.step(2)
         us = autotune.time_config(lat, shape["block"], shape["variant"], steps=200, repeats=3)

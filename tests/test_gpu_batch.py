@@ -157,3 +157,21 @@ def test_batch_of_dataset_shapes_equals_solo_solves(cuda):
     assert res[7]["diverged"] and any(r["converged"] for r in res)
     assert len(set(steps)) >= 3  # retirement interleaves
     b.close()
+
+
+@pytest.mark.parametrize("precision", ["fp32_t16", "bf16"])
+def test_batch_equals_solo_with_reduced_storage(precision, cuda):
+    """The persistent batch kernel with FP32 fluid / scaled FP16 thermal storage and with BF16 fluid storage: step
+    counts and fields equal the solo solves bit for bit."""
+    ds = small_designs()[:3]
+    run = dict(max_steps=1500, stats_every=100, tol_ke=2e-4, tol_T=2e-4)
+    with Batch(ds, precision=precision) as b:
+        res = b.run(**run)
+        got = [[t.cpu().numpy() for t in b.lattice(i).fields()] for i in range(len(ds))]
+    for i, d in enumerate(ds):
+        with Lattice(d["mask"], precision=precision, **{k: v for k, v in d.items() if k != "mask"}) as lat:
+            ref = lat.run(**run)
+            want = [t.cpu().numpy() for t in lat.fields()]
+        assert res[i]["steps"] == ref["steps"] and res[i]["converged"] == ref["converged"]
+        for a, c in zip(got[i], want):
+            assert np.array_equal(a, c)

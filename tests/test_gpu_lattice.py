@@ -1,14 +1,15 @@
 """The fused coupled step (libxac.so lattice) against the oracle's restatement of src/simulation.py.
 
 FP32 parity is bit-exact on finite inputs: identical fields after any number of steps. The 16-bit
-storage forms are measured against the FP64 oracle with stated bounds."""
+storage forms are measured against the FP64 solve on the GPU (itself bit-identical to the CPU restatement built in
+double) with stated bounds."""
 import numpy as np
 import pytest
 import torch
 
 from oracle.ref import Ref
 from xadvcool_b200 import designs
-from xadvcool_b200.lattice import Lattice
+from xadvcool_b200.lattice import Lattice, reference_run_fp64
 from xadvcool_b200.simulation import run_simulation
 
 pytestmark = pytest.mark.gpu
@@ -189,13 +190,31 @@ def test_pump_constant_power_tracks_oracle(cuda):
     assert res["u_inlet_final"] != pytest.approx(0.03, rel=1e-3)
 
 
-# Measured on B200 for the 64x32x16 finned plate after 2000 steps (relative L2 vs the FP64 oracle):
-# bf16 keeps u to 0.7% and p to 0.09%, but its 8-bit mantissa leaves T - T_in 15% off (the slowly relaxing
-# solid, tau 5.5, accumulates the rounding); fp16 is the usable 16-bit form. Bounds: 2x the measured values.
-@pytest.mark.parametrize("precision,tol_u,tol_T", [("fp16", 2e-2, 2e-2), ("bf16", 2e-2, 0.35)])
+def test_fp64_gpu_solve_equals_the_fp64_oracle(cuda):
+    """The FP64 solve on the GPU (the reference's six operators in double) against the CPU restatement built in
+    double, on config C1's finned plate with a seeded heat map: the same bits after 300 steps."""
+    mask = designs.straight_fin_plate()
+    hs = np.zeros(mask.shape, np.float32)
+    hs[:, :, 0] = np.random.default_rng(7).random(mask.shape[:2]).astype(np.float32)
+    ref = Ref(64).run_simulation(mask, max_steps=300, tol_ke=0, tol_T=0, stats_every=10 ** 9, heat_source=hs, **C1)
+    got = [t.cpu().numpy() for t in reference_run_fp64(mask, 300, heat_source=hs, **C1)]
+    for name, a, b in zip(("rho", "u", "T"), got, (ref["rho"], ref["u"], ref["T"])):
+        assert a.dtype == np.float64 and np.array_equal(a.view(np.uint64), b.view(np.uint64)), name
+
+
+def fp64_fields(mask, steps, **kw):
+    return [t.cpu().numpy() for t in reference_run_fp64(mask, steps, **kw)]
+
+
+# Measured on B200 for the 64x32x16 finned plate after 2000 steps (relative L2 vs the FP64 GPU solve): fp16 u 1.1e-3,
+# p 3.1e-4, T - T_in 8.3e-3; bf16 (fluid only; thermal in scaled FP16) u 6.9e-3, p 8.9e-4, T - T_in 9.0e-3 (with
+# BF16 thermal storage T was 15.6% off: its 8-bit significand loses the slowly relaxing solid, tau 5.5).
+# Bounds: about 2x the measured values.
+@pytest.mark.parametrize("precision,tol_u,tol_T", [("fp32_t16", 1e-4, 2e-2), ("fp16", 2e-2, 2e-2), ("bf16", 2e-2, 2e-2)])
 def test_16bit_storage_error_vs_fp64_oracle(precision, tol_u, tol_T, cuda):
     mask = designs.straight_fin_plate()
-    ref64 = Ref(64).run_simulation(mask, max_steps=2000, tol_ke=0, tol_T=0, stats_every=10 ** 9, **C1)
+    r64, u64, T64 = fp64_fields(mask, 2000, **C1)
+    ref64 = {"rho": r64, "u": u64, "T": T64}
     _, rho, u, T = lattice_fields(mask, 2000, precision=precision, **C1)
 
     def rel_l2(a, b):
@@ -209,7 +228,7 @@ def test_16bit_storage_error_vs_fp64_oracle(precision, tol_u, tol_T, cuda):
     assert e_u < tol_u and e_p < tol_u and e_T < tol_T
 
 
-@pytest.mark.parametrize("precision", ["fp32", "fp16", "bf16"])
+@pytest.mark.parametrize("precision", ["fp32", "fp32_t16", "fp16", "bf16"])
 @pytest.mark.parametrize("block", [64, 128, 256])
 def test_launch_shapes_give_identical_bits(precision, block, cuda):
     """Every block size and both visiting orders (the staged one takes its block size from the row) on a lattice
@@ -277,26 +296,31 @@ def test_autotune_picks_a_valid_shape_without_touching_results(cuda, tmp_path, m
 
 def test_16bit_storage_scalar_errors(cuda):
     """Config C3: delta_P, R_th and Nu of the 64x32x16 finned plate after 2000 steps with FP16 / BF16 population
-    storage, against the FP64 oracle and against FP32 storage. All scalars come from the same FP64 device
-    reduction (the oracle's fields rounded to float32 first: 1e-7 relative, far below the errors measured)."""
+    storage, against the FP64 GPU solve and against FP32 storage. All scalars come from the same FP64 device
+    reduction (the FP64 fields rounded to float32 first: 1e-7 relative, far below the errors measured)."""
     from xadvcool_b200.metrics import device_scalars
     mask = designs.straight_fin_plate()
-    ref64 = Ref(64).run_simulation(mask, max_steps=2000, tol_ke=0, tol_T=0, stats_every=10 ** 9, **C1)
+    r64, u64, T64 = fp64_fields(mask, 2000, **C1)
+    ref64 = {"rho": r64, "u": u64, "T": T64}
     box = dict(tau_fluid=C1["tau_fluid"], Pr=C1["Pr"], u_inlet_val=C1["u_inlet_val"], buf=8, core_nx=48, core_ny=32)
     keys = ("delta_P", "R_th", "Nu")
     s64 = device_scalars(ref64["rho"].astype(np.float32), ref64["u"].astype(np.float32),
                          ref64["T"].astype(np.float32), mask, **box)
     out = {}
-    for prec in ("fp32", "fp16", "bf16"):
+    for prec in ("fp32", "fp32_t16", "fp16", "bf16"):
         _, rho, u, T = lattice_fields(mask, 2000, precision=prec, **C1)
         out[prec] = device_scalars(rho, u, T, mask, **box)
     rel = {p: {k: abs(out[p][k] - s64[k]) / abs(s64[k]) for k in keys} for p in out}
-    rel32 = {p: {k: abs(out[p][k] - out["fp32"][k]) / abs(out["fp32"][k]) for k in keys} for p in ("fp16", "bf16")}
+    rel32 = {p: {k: abs(out[p][k] - out["fp32"][k]) / abs(out["fp32"][k]) for k in keys}
+             for p in ("fp32_t16", "fp16", "bf16")}
     print("scalar errors vs FP64:", rel, "vs FP32:", rel32)
-    # Measured on B200 (relative to FP64): fp32 delta_P 5e-6, R_th and Nu 3.7e-3 (C1's heat power 1e-4 gives a
-    # temperature rise near 1e-3 K that float32 T = 25 + rise resolves to ~1e-6 K); fp16 2.1e-4 / 6.2% / 4.1%;
-    # bf16 3.4e-4 / 50% / 170%. Bounds: 2x the measured values.
-    bounds = {"fp32": (1e-5, 8e-3, 8e-3), "fp16": (5e-4, 0.13, 0.09), "bf16": (1e-3, 1.0, 3.5)}
+    # Measured on B200: fp32 delta_P 5e-6, R_th and Nu 3.7e-3 (C1's heat power 1e-4 gives a temperature rise near
+    # 1e-3 K, which float32 T = 25 + rise resolves to ~1e-6 K); fp16 2.1e-4 / 6.2% / 4.1%; bf16 (fluid only) 3.4e-4 /
+    # 10.7% / 9.3%; fp32_t16 5e-6 / 28% / 21%. Only FP32 storage holds R_th and Nu within 1% here: a thermal
+    # population's 16-bit deviation is dominated by its advective part w_i*T*3(e_i.u) ~ 0.2, and FP16 resolves it to
+    # ~1e-4, coarser than the signal w_i*dT ~ 5e-5 of this weakly heated plate. Bounds: about 2x the measured values.
+    bounds = {"fp32": (1e-5, 8e-3, 8e-3), "fp32_t16": (1e-5, 0.56, 0.42), "fp16": (5e-4, 0.13, 0.09),
+              "bf16": (1e-3, 0.22, 0.19)}
     for p, b in bounds.items():
         for k, lim in zip(keys, b):
             assert rel[p][k] < lim, (p, k, rel[p][k])
@@ -307,7 +331,7 @@ def _rel_l2(a, b):
     return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
 
 
-@pytest.mark.parametrize("precision", ["fp16", "bf16"])
+@pytest.mark.parametrize("precision", ["fp32_t16", "fp16", "bf16"])
 @pytest.mark.parametrize("nx", [150, 180])
 def test_16bit_storage_at_row_lengths_160_and_192(nx, precision, cuda):
     """16-bit storage on a gyroid at row lengths 160 and 192 (the benchmark and dataset widths): both visiting orders
@@ -329,8 +353,8 @@ def test_16bit_storage_at_row_lengths_160_and_192(nx, precision, cuda):
     print(f"{precision} nx={nx}: rel L2 vs FP32 u {e_u:.3e} p {e_p:.3e} T {e_T:.3e}")
     # measured on B200 (both row lengths): fp16 u 8.1e-4, p 2.5e-3, T 1.6e-3; bf16 u 6.5e-3, p 1.5e-3, T 1.3e-2.
     # Bounds: about 2x those.
-    lim = {"fp16": (2e-3, 5e-3, 4e-3), "bf16": (1.5e-2, 4e-3, 3e-2)}[precision]
-    assert e_u < lim[0] and e_p < lim[1] and e_T < lim[2]
+    lim = {"fp32_t16": (0.0, 0.0, 4e-3), "fp16": (2e-3, 5e-3, 4e-3), "bf16": (1.5e-2, 4e-3, 3e-2)}[precision]
+    assert e_u <= lim[0] and e_p <= lim[1] and e_T < lim[2]  # FP32 fluid: the same fluid fields as FP32
 
 
 @pytest.mark.parametrize("precision", ["fp32", "fp16"])

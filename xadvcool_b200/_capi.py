@@ -14,8 +14,10 @@ LIB_PATH = Path(os.environ.get("XAC_LIB", _PKG / "libxac.so"))
 
 XAC_OK, XAC_EINVAL, XAC_ECUDA, XAC_EDIVERGED, XAC_ETIMEOUT, XAC_ENOMEM = range(6)
 BC_FLUID, BC_SOLID, BC_INLET, BC_OUTLET = 0, 1, 2, 3
-FP32, FP16, BF16 = 0, 1, 2
-PRECISIONS = {"fp32": FP32, "fp16": FP16, "bf16": BF16}
+FP32, FP16, BF16, FP32_T16 = 0, 1, 2, 3
+# population storage: fp32 both lattices; fp16 both lattices; bf16 fluid with FP16 thermal; fp32_t16 FP32 fluid
+# with FP16 thermal (include/xac.h gives their measured accuracy)
+PRECISIONS = {"fp32": FP32, "fp16": FP16, "bf16": BF16, "fp32_t16": FP32_T16}
 
 # stats slots (XAC_ST_*)
 ST_MAX_V, ST_SUM_V, ST_SUM_KE, ST_COUNT, ST_SUM_RHO, ST_SUM_RHO_IN, ST_SUM_RHO_OUT, ST_SUM_UX_OUT = range(8)
@@ -110,6 +112,7 @@ SIGNATURES = {
     "xac_test_periodic_stream_solids": [_vp, _vp, _vp, _i, _i, _i, _vp],
     "xac_test_couette_stream": [_vp, _vp, _vp, _f, _i, _i, _i, _vp],
     "xac_lattice_create": [C.POINTER(Desc), C.POINTER(_vp), _vp],
+    "xac_reference_run_fp64": [C.POINTER(Desc), _i, _vp, _vp, _vp, _vp],
     "xac_lattice_destroy": [_vp],
     "xac_lattice_init_fields": [_vp, _vp, _vp, _vp, _vp],
     "xac_lattice_step": [_vp, _i, _vp],

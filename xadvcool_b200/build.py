@@ -28,6 +28,7 @@ UNITS = [
     ("step_f32.cu", ["--fmad=false"]),
     ("step_f16.cu", ["--fmad=false"]),
     ("step_bf16.cu", ["--fmad=false"]),
+    ("step_f32t16.cu", ["--fmad=false"]),
     ("stats_noalloc.cu", ["--fmad=false"]),
     ("conv3d.cu", []),
     ("designs.cu", ["--fmad=false"]),

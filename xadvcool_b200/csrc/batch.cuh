@@ -105,7 +105,7 @@ __device__ __forceinline__ int find_slot_shared(const uint32_t* prefix, int lo, 
 }
 
 // tile = blockDim consecutive row positions (rows of `pitch` positions, x >= nx padding), one per thread
-template <typename S, bool kMacro, bool kOwn>
+template <typename SP, typename SQ, bool kMacro, bool kOwn>
 __device__ __forceinline__ void batch_step_tile(const BatchDesign& d, uint32_t tile, int cur) {
   const uint32_t pos = tile * blockDim.x + threadIdx.x;
   const uint32_t pitch = (uint32_t)d.p.g.pitch;
@@ -116,11 +116,12 @@ __device__ __forceinline__ void batch_step_tile(const BatchDesign& d, uint32_t t
   const uint32_t lw = valid ? __ldg(d.link + c) : ((uint32_t)kSolid << kTypeShift);
   const unsigned fluid_lanes = __ballot_sync(0xffffffffu, valid && link_type(lw) != kSolid);
   const int lane = threadIdx.x & 31;
-  coupled_cell<S, kMacro, kOwn, 1, 0>(c, pop_base(r, x, d.p.g, (int)pitch), (const S*)d.P[cur], (S*)d.P[cur ^ 1],
-                                         (const S*)d.Q[cur], (S*)d.Q[cur ^ 1], d.qsrc, d.u_in, d.rho, d.ux, d.uy,
-                                         d.uz, d.T, d.p, valid, lw, (fluid_lanes & sector_group<S>(lane)) != 0u);
-  pad_fill<S, 0>(valid, fluid_lanes, __ballot_sync(0xffffffffu, valid), lane, (S*)d.P[cur ^ 1], (S*)d.Q[cur ^ 1],
-                 pop_base(r, x, d.p.g, (int)pitch), d.p.g);
+  coupled_cell<SP, SQ, kMacro, kOwn, 1, 0>(c, pop_base(r, x, d.p.g, (int)pitch), (const SP*)d.P[cur],
+                                            (SP*)d.P[cur ^ 1], (const SQ*)d.Q[cur], (SQ*)d.Q[cur ^ 1], d.qsrc, d.u_in,
+                                            d.rho, d.ux, d.uy, d.uz, d.T, d.p, valid, lw,
+                                            (fluid_lanes & sector_group<SP>(lane)) != 0u);
+  pad_fill<SP, SQ, 0>(valid, fluid_lanes, __ballot_sync(0xffffffffu, valid), lane, (SP*)d.P[cur ^ 1],
+                      (SQ*)d.Q[cur ^ 1], pop_base(r, x, d.p.g, (int)pitch), d.p.g);
 }
 
 struct BatchRun {
@@ -133,7 +134,7 @@ struct BatchRun {
   double target_power;
 };
 
-template <typename S>
+template <typename SP, typename SQ>
 #ifndef XAC_BATCH_MIN_BLOCKS
 #define XAC_BATCH_MIN_BLOCKS 4  // at most 64 registers; 3 and 5 blocks per SM measured slower
 #endif
@@ -177,12 +178,12 @@ __global__ void __launch_bounds__(256, XAC_BATCH_MIN_BLOCKS) batch_persistent_ke
       const bool macro = stats || ls + 1 == run.max_steps;
       const int cur = (int)(ls & 1);
       if (own) {
-        if (macro) batch_step_tile<S, true, true>(d, tile, cur);
-        else batch_step_tile<S, false, true>(d, tile, cur);
+        if (macro) batch_step_tile<SP, SQ, true, true>(d, tile, cur);
+        else batch_step_tile<SP, SQ, false, true>(d, tile, cur);
       } else if (macro) {
-        batch_step_tile<S, true, false>(d, tile, cur);
+        batch_step_tile<SP, SQ, true, false>(d, tile, cur);
       } else {
-        batch_step_tile<S, false, false>(d, tile, cur);
+        batch_step_tile<SP, SQ, false, false>(d, tile, cur);
       }
     }
     if (!grid_sync(ctl, run.spin_limit)) break;
@@ -193,10 +194,10 @@ __global__ void __launch_bounds__(256, XAC_BATCH_MIN_BLOCKS) batch_persistent_ke
         const int k = find_slot(ctl->stat_prefix, na, t);
         const BatchDesign& d = D[__ldcg(ctl->active + k)];  // geometry and pointers never change
         const uint32_t tile = t - __ldcg(ctl->stat_prefix + k);
-        const S* Qnew = (const S*)d.Q[((step - d.start) & 1) ^ 1];
+        const SQ* Qnew = (const SQ*)d.Q[((step - d.start) & 1) ^ 1];
         for (uint32_t c = tile * kStatsTile + threadIdx.x; c < (tile + 1) * kStatsTile && c < d.ncell;
              c += blockDim.x)
-          d.T[c] = finalize_T_cell<S, true>(Qnew, d.link, d.p, c);
+          d.T[c] = finalize_T_cell<SQ, true>(Qnew, d.link, d.p, c);
         __syncthreads();
         FieldView v{};
         v.rho = d.rho;

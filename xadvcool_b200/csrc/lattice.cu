@@ -6,6 +6,7 @@
 #include <cstring>
 #include <map>
 #include <tuple>
+#include <type_traits>
 #include <mutex>
 #include <utility>
 #include <vector>
@@ -89,11 +90,11 @@ __global__ void import_fields_kernel(const float* __restrict__ rho_r, const floa
 
 // simulation.py:89-90 (equilibria) followed by the fluid collision of the reference's first replay
 // (simulation.py:94), which this scheme performs ahead of the first streaming step.
-template <typename S>
+template <typename SP, typename SQ>
 __global__ void init_state_kernel(const float* __restrict__ rho, const float* __restrict__ ux,
                                   const float* __restrict__ uy, const float* __restrict__ uz,
-                                  const float* __restrict__ T, const uint8_t* __restrict__ type, S* __restrict__ P0,
-                                  S* __restrict__ P1, S* __restrict__ Q0, StepParams p) {
+                                  const float* __restrict__ T, const uint8_t* __restrict__ type, SP* __restrict__ P0,
+                                  SP* __restrict__ P1, SQ* __restrict__ Q0, StepParams p) {
   const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (c >= p.g.ncell) return;
   const int RL = p.g.pitch;
@@ -110,10 +111,10 @@ __global__ void init_state_kernel(const float* __restrict__ rho, const float* __
   {                                                                                   \
     const float fe = feq_term(w_of(I) * r, edotu<I>(vx, vy, vz), usq15);             \
     const float pc = solid ? fe : fe - omega * (fe - fe);                             \
-    Pop<S>::st(P0 + e0 + (long long)I * RL, pc, w_of(I));                            \
-    Pop<S>::st(P1 + e0 + (long long)I * RL, pc, w_of(I));                            \
+    Pop<SP>::st(P0 + e0 + (long long)I * RL, pc, w_of(I));                           \
+    Pop<SP>::st(P1 + e0 + (long long)I * RL, pc, w_of(I));                           \
     const float ge = feq_term(w_of(I) * Tc, edotu<I>(tx, ty, tz), usq15t);           \
-    Pop<S>::st(Q0 + e0 + (long long)I * RL, ge, w_of(I) * p.T_ref);                  \
+    Pop<SQ>::st(Q0 + e0 + (long long)I * RL, ge, w_of(I) * p.T_ref);                 \
   }
   XAC_FOR19(XAC_INIT)
 #undef XAC_INIT
@@ -141,15 +142,16 @@ __global__ void export_fields_kernel(const float* __restrict__ rho, const float*
 
 __global__ void set_scalar_kernel(float* dst, float v) { *dst = v; }
 
-// Memory-pattern probe of the fused step: the threads, the link-word reads, the population addresses (fluid pulls
-// with the bounce-back reads its link bits select, thermal pulls from the neighbours) and the whole-sector fills
-// of solid and padding lanes that coupled_step_kernel has, with no arithmetic: every value read is stored
-// unchanged at the cell's own position of the other buffer. Its time is the floor the step's memory access
-// pattern sets. (At the domain faces the thermal rules read the cell's own row instead of a neighbour: the probe
-// pulls there too, which reads padding or guard values.)
-template <typename S, int kT>
-__global__ void __launch_bounds__(256) pattern_copy_kernel(const S* __restrict__ Pin, S* __restrict__ Pout,
-                                                           const S* __restrict__ Qin, S* __restrict__ Qout,
+// Memory-pattern probe of the fused step (SP / SQ: unsigned words of the fluid / thermal storage size): the
+// threads, the link-word reads, the population addresses (fluid pulls with the bounce-back reads its link bits
+// select, thermal pulls from the neighbours) and the whole-sector fills of solid and padding lanes that
+// coupled_step_kernel has, with no arithmetic: every value read is stored unchanged at the cell's own position of
+// the other buffer. Its time is the floor the step's memory access pattern sets. (At the domain faces the thermal
+// rules read the cell's own row instead of a neighbour: the probe pulls there too, which reads padding or guard
+// values.)
+template <typename SP, typename SQ, int kT>
+__global__ void __launch_bounds__(256) pattern_copy_kernel(const SP* __restrict__ Pin, SP* __restrict__ Pout,
+                                                           const SQ* __restrict__ Qin, SQ* __restrict__ Qout,
                                                            const uint32_t* __restrict__ link, Geom g,
                                                            uint32_t reverse) {
   const int RL = row_len<kT>(g);
@@ -162,38 +164,42 @@ __global__ void __launch_bounds__(256) pattern_copy_kernel(const S* __restrict__
   const uint32_t c = r * (uint32_t)g.nx + x;
   const uint32_t lw = valid ? __ldg(link + c) : ((uint32_t)kSolid << kTypeShift);
   const bool fluid = valid && link_type(lw) != kSolid;
-  const unsigned grp = sector_group<S>(lane);
-  const bool fill_p = (__ballot_sync(0xffffffffu, fluid) & grp) != 0u;
-  const bool fill_q = (__ballot_sync(0xffffffffu, valid) & grp) != 0u;
+  const bool fill_p = (__ballot_sync(0xffffffffu, fluid) & sector_group<SP>(lane)) != 0u;
+  const bool fill_q = (__ballot_sync(0xffffffffu, valid) & sector_group<SQ>(lane)) != 0u;
   const uint32_t e0 = pop_base(r, x, g, RL);
-  const S zero = static_cast<S>(0.0f);
   if (fluid) {
-    const Rows<S, kT> P = rows_at<kT>(Pin, e0, g, RL);
+    const Rows<SP, kT> P = rows_at<kT>(Pin, e0, g, RL);
 #define XAC_PC_P(I) Pout[e0 + (I) * RL] = ((lw >> (I)) & 1u) ? __ldg(P.own(opp_of(I))) : __ldg(P.template pull<I>());
     XAC_FOR19(XAC_PC_P)
 #undef XAC_PC_P
   } else if (fill_p) {
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) Pout[e0 + i * RL] = zero;
+    for (int i = 0; i < kQ; ++i) Pout[e0 + i * RL] = SP{};
   }
   if (valid) {
-    const Rows<S, kT> Q = rows_at<kT>(Qin, e0, g, RL);
+    const Rows<SQ, kT> Q = rows_at<kT>(Qin, e0, g, RL);
 #define XAC_PC_Q(I) Qout[e0 + (I) * RL] = __ldg(Q.template pull<I>());
     XAC_FOR19(XAC_PC_Q)
 #undef XAC_PC_Q
   } else if (fill_q) {
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) Qout[e0 + i * RL] = zero;
+    for (int i = 0; i < kQ; ++i) Qout[e0 + i * RL] = SQ{};
   }
 }
 
-template <typename S>
+// The probe moves bits only: each storage type is copied as the unsigned word of its size.
+template <size_t kBytes>
+using RawWord = typename std::conditional<kBytes == 4, unsigned int, unsigned short>::type;
+
+template <typename SP0, typename SQ0>
 void launch_pattern_copy(const void* Pin, void* Pout, const void* Qin, void* Qout, const uint32_t* link, const Geom& g,
                          int block, uint32_t reverse, cudaStream_t s) {
+  using SP = RawWord<sizeof(SP0)>;
+  using SQ = RawWord<sizeof(SQ0)>;
   const unsigned grid = (unsigned)(((long long)g.rows * g.pitch + block - 1) / block);
 #define XAC_PC(KT)                                                                                                 \
-  pattern_copy_kernel<S, KT><<<grid, block, 0, s>>>((const S*)Pin, (S*)Pout, (const S*)Qin, (S*)Qout, link, g, \
-                                                    reverse)
+  pattern_copy_kernel<SP, SQ, KT><<<grid, block, 0, s>>>((const SP*)Pin, (SP*)Pout, (const SQ*)Qin, (SQ*)Qout, \
+                                                          link, g, reverse)
   switch (g.pitch) {
     case 32: XAC_PC(32); break;
     case 64: XAC_PC(64); break;
@@ -290,7 +296,7 @@ static __global__ void run_decision_kernel(const double* __restrict__ st, RunCtl
 struct LatticeImpl {
   Geom g{};
   int precision = XAC_FP32;
-  size_t pop_elem = 4;
+  size_t p_elem = 4, q_elem = 4;  // bytes per fluid / thermal population
   double tau_fluid = 0.6, Pr = 7.0, k_ratio = 628.0, u_inlet_nominal = 0.03, rho_outlet = 1.0, t_inlet = 25.0,
          heat_power = 0.1;
   float tau_th_f = 0.5f, tau_th_s = 0.5f;
@@ -381,25 +387,33 @@ struct LatticeImpl {
     if (capture) cudaStreamDestroy(capture);
   }
 
-  template <typename S>
+  template <int kPrec>
   int launch_step(cudaStream_t s, bool macro, bool own) {
     const StepParams p = params();
-    const S* Pin = (const S*)P[cur];
-    S* Pout = (S*)P[cur ^ 1];
-    const S* Qin = (const S*)Qb[cur];
-    S* Qout = (S*)Qb[cur ^ 1];
-    StepLaunch a{Pin, Pout, Qin, Qout, link, qsrc, u_in, rho, ux, uy, uz, T, p, tune_block, tune_variant, macro, own, s};
-    launch_coupled_step<S>(a);
+    StepLaunch a{P[cur], P[cur ^ 1], Qb[cur], Qb[cur ^ 1], link, qsrc, u_in, rho, ux, uy, uz, T, p, tune_block,
+                 tune_variant, macro, own, s};
+    launch_coupled_step<typename Storage<kPrec>::P, typename Storage<kPrec>::Q>(a);
     cur ^= 1;
     return XAC_OK;
   }
 
   int launch_step_any(cudaStream_t s, bool macro, bool own) {
     switch (precision) {
-      case XAC_FP16: return launch_step<__half>(s, macro, own);
-      case XAC_BF16: return launch_step<__nv_bfloat16>(s, macro, own);
-      default: return launch_step<float>(s, macro, own);
+      case XAC_FP16: return launch_step<XAC_FP16>(s, macro, own);
+      case XAC_BF16: return launch_step<XAC_BF16>(s, macro, own);
+      case XAC_FP32_T16: return launch_step<XAC_FP32_T16>(s, macro, own);
+      default: return launch_step<XAC_FP32>(s, macro, own);
     }
+  }
+
+  // T of the current state into the T field (the thermal populations' storage type follows the precision mode)
+  void launch_finalize_T(cudaStream_t s) {
+    const StepParams p = params();
+    const unsigned grid = grid_for(g.ncell, kBlock);
+    if (precision == XAC_FP32)
+      thermal_finalize_kernel<float><<<grid, kBlock, 0, s>>>((const float*)Qb[cur], link, T, p);
+    else
+      thermal_finalize_kernel<__half><<<grid, kBlock, 0, s>>>((const __half*)Qb[cur], link, T, p);
   }
 
   // n plain steps (no own step), the last one writing rho/u
@@ -499,19 +513,7 @@ struct LatticeImpl {
       return cuda_status(e, "run loop graph");
     }
     launch_plain(capture, every);
-    const StepParams p = params();
-    const unsigned grid = grid_for(g.ncell, kBlock);
-    switch (precision) {
-      case XAC_FP16:
-        thermal_finalize_kernel<__half><<<grid, kBlock, 0, capture>>>((const __half*)Qb[cur], link, T, p);
-        break;
-      case XAC_BF16:
-        thermal_finalize_kernel<__nv_bfloat16><<<grid, kBlock, 0, capture>>>((const __nv_bfloat16*)Qb[cur], link,
-                                                                             T, p);
-        break;
-      default:
-        thermal_finalize_kernel<float><<<grid, kBlock, 0, capture>>>((const float*)Qb[cur], link, T, p);
-    }
+    launch_finalize_T(capture);
     const auto spec = stats_spec();
     const int ntiles = (int)stats_tiles(g.ncell);
     stats_partials_kernel<<<ntiles, kStatsBlock, 0, capture>>>(view(), spec, rows);
@@ -531,18 +533,7 @@ struct LatticeImpl {
 
   int finalize_T(cudaStream_t s) {
     if (T_step == step) return XAC_OK;
-    const StepParams p = params();
-    const unsigned grid = grid_for(g.ncell, kBlock);
-    switch (precision) {
-      case XAC_FP16:
-        thermal_finalize_kernel<__half><<<grid, kBlock, 0, s>>>((const __half*)Qb[cur], link, T, p);
-        break;
-      case XAC_BF16:
-        thermal_finalize_kernel<__nv_bfloat16><<<grid, kBlock, 0, s>>>((const __nv_bfloat16*)Qb[cur], link, T, p);
-        break;
-      default:
-        thermal_finalize_kernel<float><<<grid, kBlock, 0, s>>>((const float*)Qb[cur], link, T, p);
-    }
+    launch_finalize_T(s);
     XAC_CUDA(cudaGetLastError());
     T_step = step;
     return XAC_OK;
@@ -698,7 +689,8 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
   XAC_REQUIRE(d->mask, "xac_lattice_create: null mask");
   XAC_REQUIRE(d->tau_fluid > 0.5, "xac_lattice_create: tau_fluid must exceed 0.5 (got %g)", d->tau_fluid);
   XAC_REQUIRE(d->Pr > 0, "xac_lattice_create: Pr must be positive");
-  XAC_REQUIRE(d->precision == XAC_FP32 || d->precision == XAC_FP16 || d->precision == XAC_BF16,
+  XAC_REQUIRE(d->precision == XAC_FP32 || d->precision == XAC_FP16 || d->precision == XAC_BF16 ||
+                  d->precision == XAC_FP32_T16,
               "xac_lattice_create: unknown precision %d", d->precision);
   const int nx = d->nx, ny = d->ny, nz = d->nz;
   const long long n = (long long)nx * ny * nz;
@@ -711,7 +703,8 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
   L.g.guard = (long long)(ny + 2) * kQ * L.g.pitch;
   L.g.N = (long long)L.g.rows * kQ * L.g.pitch + 2 * L.g.guard;
   L.precision = d->precision;
-  L.pop_elem = d->precision == XAC_FP32 ? 4 : 2;
+  L.p_elem = (d->precision == XAC_FP32 || d->precision == XAC_FP32_T16) ? 4 : 2;
+  L.q_elem = d->precision == XAC_FP32 ? 4 : 2;
   L.tau_fluid = d->tau_fluid;
   L.Pr = d->Pr;
   L.k_ratio = d->k_ratio;
@@ -736,10 +729,10 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
         type[((size_t)z * ny + y) * nx + x] = (uint8_t)m;
       }
   std::vector<float> q = host_qsrc(d);
-  const size_t pop_bytes = (size_t)L.g.N * L.pop_elem;
+  const size_t p_bytes = (size_t)L.g.N * L.p_elem, q_bytes = (size_t)L.g.N * L.q_elem;
   for (int b = 0; b < 2; ++b) {
-    XAC_CUDA(cudaMalloc(&L.P[b], pop_bytes));
-    XAC_CUDA(cudaMalloc(&L.Qb[b], pop_bytes));
+    XAC_CUDA(cudaMalloc(&L.P[b], p_bytes));
+    XAC_CUDA(cudaMalloc(&L.Qb[b], q_bytes));
   }
   int r;
   if ((r = dmalloc(&L.type, n, "alloc type")) != XAC_OK) return r;
@@ -759,8 +752,8 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
   XAC_CUDA(cudaMallocHost(&L.host_out, 64 * sizeof(double)));
   // guards and row padding are never used as values; keep them defined
   for (int b = 0; b < 2; ++b) {
-    XAC_CUDA(cudaMemsetAsync(L.P[b], 0, pop_bytes, s));
-    XAC_CUDA(cudaMemsetAsync(L.Qb[b], 0, pop_bytes, s));
+    XAC_CUDA(cudaMemsetAsync(L.P[b], 0, p_bytes, s));
+    XAC_CUDA(cudaMemsetAsync(L.Qb[b], 0, q_bytes, s));
   }
   XAC_CUDA(cudaMemcpyAsync(L.type, type.data(), n, cudaMemcpyHostToDevice, s));
   XAC_CUDA(cudaMemcpyAsync(L.qsrc, q.data(), n * sizeof(float), cudaMemcpyHostToDevice, s));
@@ -781,17 +774,24 @@ int init_impl(LatticeImpl& L, const float* rho, const float* u, const float* T, 
   const StepParams p = L.params();
   switch (L.precision) {
     case XAC_FP16:
-      init_state_kernel<__half><<<grid, kBlock, 0, s>>>(L.rho, L.ux, L.uy, L.uz, L.T, L.type, (__half*)L.P[0],
-                                                        (__half*)L.P[1], (__half*)L.Qb[0], p);
+      init_state_kernel<__half, __half><<<grid, kBlock, 0, s>>>(L.rho, L.ux, L.uy, L.uz, L.T, L.type,
+                                                                      (__half*)L.P[0], (__half*)L.P[1],
+                                                                      (__half*)L.Qb[0], p);
       break;
     case XAC_BF16:
-      init_state_kernel<__nv_bfloat16><<<grid, kBlock, 0, s>>>(L.rho, L.ux, L.uy, L.uz, L.T, L.type,
-                                                               (__nv_bfloat16*)L.P[0], (__nv_bfloat16*)L.P[1],
-                                                               (__nv_bfloat16*)L.Qb[0], p);
+      init_state_kernel<__nv_bfloat16, __half><<<grid, kBlock, 0, s>>>(L.rho, L.ux, L.uy, L.uz, L.T, L.type,
+                                                                             (__nv_bfloat16*)L.P[0],
+                                                                             (__nv_bfloat16*)L.P[1],
+                                                                             (__half*)L.Qb[0], p);
+      break;
+    case XAC_FP32_T16:
+      init_state_kernel<float, __half><<<grid, kBlock, 0, s>>>(L.rho, L.ux, L.uy, L.uz, L.T, L.type,
+                                                                     (float*)L.P[0], (float*)L.P[1],
+                                                                     (__half*)L.Qb[0], p);
       break;
     default:
-      init_state_kernel<float><<<grid, kBlock, 0, s>>>(L.rho, L.ux, L.uy, L.uz, L.T, L.type, (float*)L.P[0],
-                                                       (float*)L.P[1], (float*)L.Qb[0], p);
+      init_state_kernel<float, float><<<grid, kBlock, 0, s>>>(L.rho, L.ux, L.uy, L.uz, L.T, L.type, (float*)L.P[0],
+                                                               (float*)L.P[1], (float*)L.Qb[0], p);
   }
   XAC_CUDA(cudaGetLastError());
   L.cur = 0;
@@ -927,13 +927,18 @@ int xac_lattice_pattern_copy(xac_lattice* lat, int launches, double* us_per_laun
     const int c = k & 1;
     switch (L.precision) {
       case XAC_FP16:
-        launch_pattern_copy<__half>(L.P[c], L.P[c ^ 1], L.Qb[c], L.Qb[c ^ 1], L.link, L.g, L.tune_block, c, s);
+        launch_pattern_copy<__half, __half>(L.P[c], L.P[c ^ 1], L.Qb[c], L.Qb[c ^ 1], L.link, L.g, L.tune_block, c, s);
         break;
       case XAC_BF16:
-        launch_pattern_copy<__nv_bfloat16>(L.P[c], L.P[c ^ 1], L.Qb[c], L.Qb[c ^ 1], L.link, L.g, L.tune_block, c, s);
+        launch_pattern_copy<__nv_bfloat16, __half>(L.P[c], L.P[c ^ 1], L.Qb[c], L.Qb[c ^ 1], L.link, L.g,
+                                                        L.tune_block, c, s);
+        break;
+      case XAC_FP32_T16:
+        launch_pattern_copy<float, __half>(L.P[c], L.P[c ^ 1], L.Qb[c], L.Qb[c ^ 1], L.link, L.g, L.tune_block, c,
+                                                s);
         break;
       default:
-        launch_pattern_copy<float>(L.P[c], L.P[c ^ 1], L.Qb[c], L.Qb[c ^ 1], L.link, L.g, L.tune_block, c, s);
+        launch_pattern_copy<float, float>(L.P[c], L.P[c ^ 1], L.Qb[c], L.Qb[c ^ 1], L.link, L.g, L.tune_block, c, s);
     }
   };
   for (int k = 0; k < 4; ++k) launch(k);  // warm-up
@@ -1027,8 +1032,7 @@ int xac_lattice_validate(xac_lattice* lat, double* out_host, void* stream) {
 int xac_lattice_state_bytes(const xac_lattice* lat, size_t* bytes) {
   XAC_REQUIRE(lat && bytes, "xac_lattice_state_bytes: null pointer");
   const LatticeImpl& L = lat->impl;
-  const size_t pop = (size_t)L.g.N * L.pop_elem;
-  *bytes = 64 + 2 * pop + 5 * (size_t)L.g.ncell * sizeof(float);
+  *bytes = 64 + (size_t)L.g.N * (L.p_elem + L.q_elem) + 5 * (size_t)L.g.ncell * sizeof(float);
   return XAC_OK;
 }
 
@@ -1048,13 +1052,13 @@ int xac_lattice_save_state(xac_lattice* lat, void* host_dst, size_t bytes, void*
   std::memcpy(&hdr[7], &u_in, sizeof(float));
   char* dst = (char*)host_dst;
   std::memcpy(dst, hdr, 64);
-  const size_t pop = (size_t)L.g.N * L.pop_elem;
+  const size_t pb = (size_t)L.g.N * L.p_elem, qb = (size_t)L.g.N * L.q_elem;
   const size_t nf = (size_t)L.g.ncell * sizeof(float);
-  XAC_CUDA(cudaMemcpyAsync(dst + 64, L.P[L.cur], pop, cudaMemcpyDeviceToHost, s));
-  XAC_CUDA(cudaMemcpyAsync(dst + 64 + pop, L.Qb[L.cur], pop, cudaMemcpyDeviceToHost, s));
+  XAC_CUDA(cudaMemcpyAsync(dst + 64, L.P[L.cur], pb, cudaMemcpyDeviceToHost, s));
+  XAC_CUDA(cudaMemcpyAsync(dst + 64 + pb, L.Qb[L.cur], qb, cudaMemcpyDeviceToHost, s));
   const float* f[5] = {L.rho, L.ux, L.uy, L.uz, L.T};
   for (int k = 0; k < 5; ++k)
-    XAC_CUDA(cudaMemcpyAsync(dst + 64 + 2 * pop + k * nf, f[k], nf, cudaMemcpyDeviceToHost, s));
+    XAC_CUDA(cudaMemcpyAsync(dst + 64 + pb + qb + k * nf, f[k], nf, cudaMemcpyDeviceToHost, s));
   XAC_CUDA(cudaStreamSynchronize(s));
   return XAC_OK;
 }
@@ -1073,15 +1077,15 @@ int xac_lattice_load_state(xac_lattice* lat, const void* host_src, size_t bytes,
   std::lock_guard<std::mutex> g(L.mu);
   cudaStream_t s = as_stream(stream);
   const char* src = (const char*)host_src;
-  const size_t pop = (size_t)L.g.N * L.pop_elem;
+  const size_t pb = (size_t)L.g.N * L.p_elem, qb = (size_t)L.g.N * L.q_elem;
   const size_t nf = (size_t)L.g.ncell * sizeof(float);
   // solid cells are read from either buffer, so both get the saved fluid populations
-  XAC_CUDA(cudaMemcpyAsync(L.P[0], src + 64, pop, cudaMemcpyHostToDevice, s));
-  XAC_CUDA(cudaMemcpyAsync(L.P[1], src + 64, pop, cudaMemcpyHostToDevice, s));
-  XAC_CUDA(cudaMemcpyAsync(L.Qb[0], src + 64 + pop, pop, cudaMemcpyHostToDevice, s));
+  XAC_CUDA(cudaMemcpyAsync(L.P[0], src + 64, pb, cudaMemcpyHostToDevice, s));
+  XAC_CUDA(cudaMemcpyAsync(L.P[1], src + 64, pb, cudaMemcpyHostToDevice, s));
+  XAC_CUDA(cudaMemcpyAsync(L.Qb[0], src + 64 + pb, qb, cudaMemcpyHostToDevice, s));
   float* f[5] = {L.rho, L.ux, L.uy, L.uz, L.T};
   for (int k = 0; k < 5; ++k)
-    XAC_CUDA(cudaMemcpyAsync(f[k], src + 64 + 2 * pop + k * nf, nf, cudaMemcpyHostToDevice, s));
+    XAC_CUDA(cudaMemcpyAsync(f[k], src + 64 + pb + qb + k * nf, nf, cudaMemcpyHostToDevice, s));
   float u_in;
   std::memcpy(&u_in, &hdr[7], sizeof(float));
   L.u_in_host = u_in;
@@ -1396,12 +1400,12 @@ struct xac_batch {
 
 namespace {
 
-template <typename S>
+template <typename SP, typename SQ>
 int batch_launch(xac_batch* b, const BatchRun& run, cudaStream_t s, bool use_graph) {
   int dev = 0, sms = 0, per_sm = 0;
   XAC_CUDA(cudaGetDevice(&dev));
   XAC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  XAC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_persistent_kernel<S>, b->block, 0));
+  XAC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_persistent_kernel<SP, SQ>, b->block, 0));
   XAC_REQUIRE(per_sm > 0, "xac_batch_run: the persistent kernel does not fit on an SM with %d threads", b->block);
   const int grid = sms * per_sm;  // every block resident: the grid barrier cannot deadlock
   BatchDesign* D = b->dD;
@@ -1428,7 +1432,7 @@ int batch_launch(xac_batch* b, const BatchRun& run, cudaStream_t s, bool use_gra
       cudaGraph_t graph = nullptr;
       cfg.stream = b->capture;
       XAC_CUDA(cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal));
-      cudaError_t le = cudaLaunchKernelExC(&cfg, (const void*)batch_persistent_kernel<S>, args);
+      cudaError_t le = cudaLaunchKernelExC(&cfg, (const void*)batch_persistent_kernel<SP, SQ>, args);
       cudaError_t ce = cudaStreamEndCapture(b->capture, &graph);
       cudaGraphExec_t exec = nullptr;
       if (le == cudaSuccess && ce == cudaSuccess && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
@@ -1449,16 +1453,17 @@ int batch_launch(xac_batch* b, const BatchRun& run, cudaStream_t s, bool use_gra
     }
   }
   cfg.stream = s;
-  XAC_CUDA(cudaLaunchKernelExC(&cfg, (const void*)batch_persistent_kernel<S>, args));
+  XAC_CUDA(cudaLaunchKernelExC(&cfg, (const void*)batch_persistent_kernel<SP, SQ>, args));
   ++b->direct_launches;
   return XAC_OK;
 }
 
 int batch_launch_any(xac_batch* b, const BatchRun& run, cudaStream_t s, bool use_graph) {
   switch (b->precision) {
-    case XAC_FP16: return batch_launch<__half>(b, run, s, use_graph);
-    case XAC_BF16: return batch_launch<__nv_bfloat16>(b, run, s, use_graph);
-    default: return batch_launch<float>(b, run, s, use_graph);
+    case XAC_FP16: return batch_launch<__half, __half>(b, run, s, use_graph);
+    case XAC_BF16: return batch_launch<__nv_bfloat16, __half>(b, run, s, use_graph);
+    case XAC_FP32_T16: return batch_launch<float, __half>(b, run, s, use_graph);
+    default: return batch_launch<float, float>(b, run, s, use_graph);
   }
 }
 
@@ -1672,7 +1677,7 @@ int xac_batch_launch_counts(const xac_batch* b, long long* graph_launches, long 
 
 int xac_batch_open(int precision, xac_batch** out) {
   XAC_REQUIRE(out, "xac_batch_open: null pointer");
-  XAC_REQUIRE(precision == XAC_FP32 || precision == XAC_FP16 || precision == XAC_BF16,
+  XAC_REQUIRE(precision == XAC_FP32 || precision == XAC_FP16 || precision == XAC_BF16 || precision == XAC_FP32_T16,
               "xac_batch_open: unknown precision %d", precision);
   *out = nullptr;
   xac_batch* b = new (std::nothrow) xac_batch();
@@ -1839,9 +1844,10 @@ int xac_lattice_footprint(const xac_desc* d, unsigned long long* bytes) {
   const long long n = (long long)d->nx * d->ny * d->nz;
   const long long pitch = (d->nx + 31) / 32 * 32;
   const long long N = ((long long)d->ny * d->nz + 2LL * (d->ny + 2)) * kQ * pitch;
-  const long long elem = d->precision == XAC_FP32 ? 4 : 2;
+  const long long p_elem = (d->precision == XAC_FP32 || d->precision == XAC_FP32_T16) ? 4 : 2;
+  const long long q_elem = d->precision == XAC_FP32 ? 4 : 2;
   const long long metric_rows = (long long)reduction_blocks(n) * kNMetrics, stat_rows = stats_tiles(n) * kNStats;
-  *bytes = (unsigned long long)(4 * N * elem + n * (1 + 4 + 4 + 5 * 4) +
+  *bytes = (unsigned long long)(2 * N * (p_elem + q_elem) + n * (1 + 4 + 4 + 5 * 4) +
                                 8 * (metric_rows > stat_rows ? metric_rows : stat_rows) + 64 * 8 + 64);
   return XAC_OK;
 }

@@ -101,6 +101,32 @@ struct Pop<__nv_bfloat16> {
     *p = __float2bfloat16_rn(v - base);
   }
 };
+// Storage of each precision mode: fluid populations P, thermal populations Q. BF16's 8-bit significand is used for
+// the fluid lattice only: a thermal population's deviation from w_i*T_inlet is dominated by its advective part
+// w_i*T*3(e_i.u) (~0.2 at T = 25, |u| = 0.05), so the temperature signal w_i*(T - T_inlet) must be resolved far
+// below it, which FP16's 11-bit significand does to ~1e-4 and BF16's 8 bits do not.
+template <int kPrecision>
+struct Storage;
+template <>
+struct Storage<XAC_FP32> {
+  using P = float;
+  using Q = float;
+};
+template <>
+struct Storage<XAC_FP16> {
+  using P = __half;
+  using Q = __half;
+};
+template <>
+struct Storage<XAC_BF16> {
+  using P = __nv_bfloat16;
+  using Q = __half;
+};
+template <>
+struct Storage<XAC_FP32_T16> {
+  using P = float;
+  using Q = __half;
+};
 
 struct StepParams {
   Geom g;
@@ -382,10 +408,10 @@ __device__ __forceinline__ void thermal_cell(const uint32_t c, const Acc& Q, S* 
 #undef XAC_TCOLLIDE
 }
 
-// cell c (compact index) whose populations start at element e0 of each array
-template <typename S, bool kMacro, bool kOwn, int kLd, int kT>
-__device__ __forceinline__ void coupled_cell(const uint32_t c, const uint32_t e0, const S* __restrict__ Pin,
-                                             S* __restrict__ Pout, const S* __restrict__ Qin, S* __restrict__ Qout,
+// cell c (compact index) whose populations start at element e0 of each array; SP / SQ: fluid / thermal storage
+template <typename SP, typename SQ, bool kMacro, bool kOwn, int kLd, int kT>
+__device__ __forceinline__ void coupled_cell(const uint32_t c, const uint32_t e0, const SP* __restrict__ Pin,
+                                             SP* __restrict__ Pout, const SQ* __restrict__ Qin, SQ* __restrict__ Qout,
                                              const float* __restrict__ qsrc, const float* __restrict__ u_in_ptr,
                                              float* __restrict__ rho_o, float* __restrict__ ux_o,
                                              float* __restrict__ uy_o, float* __restrict__ uz_o,
@@ -395,39 +421,38 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const uint32_t e0
   const bool fluid = valid && link_type(lw) != kSolid;
   float ux = 0.0f, uy = 0.0f, uz = 0.0f;
   if (fluid)
-    fluid_cell<S, kMacro, kLd, kT>(c, rows_at<kT>(Pin, e0, p.g, RL), Pout + e0, u_in_ptr, rho_o, ux_o, uy_o, uz_o, p,
-                                   lw, ux, uy, uz);
+    fluid_cell<SP, kMacro, kLd, kT>(c, rows_at<kT>(Pin, e0, p.g, RL), Pout + e0, u_in_ptr, rho_o, ux_o, uy_o, uz_o,
+                                    p, lw, ux, uy, uz);
   else if (valid)
-    solid_cell<S, kMacro, kLd, kT>(c, rows_at<kT>(Pin, e0, p.g, RL), Pout + e0, rho_o, ux_o, uy_o, uz_o, p,
-                                   fill_solid);
+    solid_cell<SP, kMacro, kLd, kT>(c, rows_at<kT>(Pin, e0, p.g, RL), Pout + e0, rho_o, ux_o, uy_o, uz_o, p,
+                                    fill_solid);
   if (!valid) return;
-  thermal_cell<S, kOwn, kLd, kT>(c, rows_at<kT>(Qin, e0, p.g, RL), Qout + e0, qsrc, T0, p, lw, ux, uy, uz);
+  thermal_cell<SQ, kOwn, kLd, kT>(c, rows_at<kT>(Qin, e0, p.g, RL), Qout + e0, qsrc, T0, p, lw, ux, uy, uz);
 }
 
 // Padding positions (x >= nx) of a row's last, partly valid sector store a value too, so that the sector is
 // written whole (no read-modify-write in L2); the values are never read.
-template <typename S, int kT>
+template <typename SP, typename SQ, int kT>
 __device__ __forceinline__ void pad_fill(bool valid, unsigned fluid_lanes, unsigned valid_lanes, int lane,
-                                         S* __restrict__ Pout, S* __restrict__ Qout, uint32_t e0, const Geom& g) {
+                                         SP* __restrict__ Pout, SQ* __restrict__ Qout, uint32_t e0, const Geom& g) {
   if (valid) return;
   const int RL = row_len<kT>(g);
-  const unsigned grp = sector_group<S>(lane);
-  if (fluid_lanes & grp) {
+  if (fluid_lanes & sector_group<SP>(lane)) {
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) Pop<S>::st(Pout + e0 + i * RL, w_of(i), w_of(i));
+    for (int i = 0; i < kQ; ++i) Pop<SP>::st(Pout + e0 + i * RL, w_of(i), w_of(i));
   }
-  if (valid_lanes & grp) {
+  if (valid_lanes & sector_group<SQ>(lane)) {
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) Pop<S>::st(Qout + e0 + i * RL, 0.0f, 0.0f);
+    for (int i = 0; i < kQ; ++i) Pop<SQ>::st(Qout + e0 + i * RL, 0.0f, 0.0f);
   }
 }
 
 // One thread per row position: block-consecutive threads walk x along a row (a warp never spans two rows, the
 // row length being a multiple of 32); positions x >= nx are padding. kT > 0 makes the row length and every
 // population offset compile-time constants; kT = 0 reads it from the geometry.
-template <typename S, bool kMacro, bool kOwn, int kT>
-__global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__ Pin, S* __restrict__ Pout,
-                                                           const S* __restrict__ Qin, S* __restrict__ Qout,
+template <typename SP, typename SQ, bool kMacro, bool kOwn, int kT>
+__global__ void __launch_bounds__(256) coupled_step_kernel(const SP* __restrict__ Pin, SP* __restrict__ Pout,
+                                                           const SQ* __restrict__ Qin, SQ* __restrict__ Qout,
                                                            const uint32_t* __restrict__ link,
                                                            const float* __restrict__ qsrc,
                                                            const float* __restrict__ u_in_ptr,
@@ -444,11 +469,11 @@ __global__ void __launch_bounds__(256) coupled_step_kernel(const S* __restrict__
   const uint32_t c = r * (uint32_t)p.g.nx + x;
   const uint32_t lw = valid ? __ldg(link + c) : ((uint32_t)kSolid << kTypeShift);
   const unsigned fluid_lanes = __ballot_sync(0xffffffffu, valid && link_type(lw) != kSolid);
-  coupled_cell<S, kMacro, kOwn, 0, kT>(c, pop_base(r, x, p.g, RL), Pin, Pout, Qin, Qout, qsrc, u_in_ptr, rho_o,
-                                           ux_o, uy_o, uz_o, T0, p, valid, lw,
-                                           (fluid_lanes & sector_group<S>(lane)) != 0u);
-  pad_fill<S, kT>(valid, fluid_lanes, __ballot_sync(0xffffffffu, valid), lane, Pout, Qout, pop_base(r, x, p.g, RL),
-                  p.g);
+  coupled_cell<SP, SQ, kMacro, kOwn, 0, kT>(c, pop_base(r, x, p.g, RL), Pin, Pout, Qin, Qout, qsrc, u_in_ptr, rho_o,
+                                            ux_o, uy_o, uz_o, T0, p, valid, lw,
+                                            (fluid_lanes & sector_group<SP>(lane)) != 0u);
+  pad_fill<SP, SQ, kT>(valid, fluid_lanes, __ballot_sync(0xffffffffu, valid), lane, Pout, Qout,
+                       pop_base(r, x, p.g, RL), p.g);
 }
 
 // ---- thermal rows staged in shared memory (launch variant 1) ------------------------------------------
@@ -496,18 +521,18 @@ __device__ __forceinline__ bool bar_wait_bounded(uint32_t bar, uint32_t parity, 
   return false;
 }
 
-template <typename S, bool kMacro, bool kOwn, int kT>
-__global__ void __launch_bounds__(kT) coupled_qstage_kernel(const S* __restrict__ Pin, S* __restrict__ Pout,
-                                                            const S* __restrict__ Qin, S* __restrict__ Qout,
+template <typename SP, typename SQ, bool kMacro, bool kOwn, int kT>
+__global__ void __launch_bounds__(kT) coupled_qstage_kernel(const SP* __restrict__ Pin, SP* __restrict__ Pout,
+                                                            const SQ* __restrict__ Qin, SQ* __restrict__ Qout,
                                                             const uint32_t* __restrict__ link,
                                                             const float* __restrict__ qsrc,
                                                             const float* __restrict__ u_in_ptr,
                                                             float* __restrict__ rho_o, float* __restrict__ ux_o,
                                                             float* __restrict__ uy_o, float* __restrict__ uz_o,
                                                             const float* __restrict__ T0, StepParams p) {
-  using St = StageQ<S, kT>;
+  using St = StageQ<SQ, kT>;
   extern __shared__ __align__(16) unsigned char sm_raw[];
-  S* sq = reinterpret_cast<S*>(sm_raw);
+  SQ* sq = reinterpret_cast<SQ*>(sm_raw);
   __shared__ __align__(8) uint64_t bar;
   const uint32_t r = p.reverse ? gridDim.x - 1u - blockIdx.x : blockIdx.x, x = threadIdx.x;
   const int lane = x & 31;
@@ -518,9 +543,9 @@ __global__ void __launch_bounds__(kT) coupled_qstage_kernel(const S* __restrict_
   }
   __syncthreads();
   if (x == 0) {
-    const uint32_t run = (uint32_t)(kT * sizeof(S));
+    const uint32_t run = (uint32_t)(kT * sizeof(SQ));
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"((kQ + 16) * run) : "memory");
-    const S* row0 = Qin + p.g.guard;
+    const SQ* row0 = Qin + p.g.guard;
     bulk_copy(sh_addr(sq + St::kPad), row0 + (long long)r * kQ * kT, kQ * run, b);
 #pragma unroll
     for (int i = 3; i < kQ; ++i) {
@@ -535,21 +560,21 @@ __global__ void __launch_bounds__(kT) coupled_qstage_kernel(const S* __restrict_
   const uint32_t e0 = pop_base(r, x, p.g, kT);
   float ux = 0.0f, uy = 0.0f, uz = 0.0f;
   if (valid && link_type(lw) != kSolid)
-    fluid_cell<S, kMacro, 0, kT>(c, rows_at<kT>(Pin, e0, p.g, kT), Pout + e0, u_in_ptr, rho_o, ux_o, uy_o, uz_o, p,
+    fluid_cell<SP, kMacro, 0, kT>(c, rows_at<kT>(Pin, e0, p.g, kT), Pout + e0, u_in_ptr, rho_o, ux_o, uy_o, uz_o, p,
                                  lw, ux, uy, uz);
   else if (valid)
-    solid_cell<S, kMacro, 0, kT>(c, rows_at<kT>(Pin, e0, p.g, kT), Pout + e0, rho_o, ux_o, uy_o, uz_o, p,
-                                 (fluid_lanes & sector_group<S>(lane)) != 0u);
+    solid_cell<SP, kMacro, 0, kT>(c, rows_at<kT>(Pin, e0, p.g, kT), Pout + e0, rho_o, ux_o, uy_o, uz_o, p,
+                                 (fluid_lanes & sector_group<SP>(lane)) != 0u);
   const bool ok = bar_wait_bounded(b, 0);
   if (!ok && x == 0) atomicOr(p.status, 1u);
   if (valid && ok)
-    thermal_cell<S, kOwn, 2, kT>(c, SmemRows<S, kT>{sq + St::kPad + x, sq + St::kOwn + St::kPad + x}, Qout + e0,
+    thermal_cell<SQ, kOwn, 2, kT>(c, SmemRows<SQ, kT>{sq + St::kPad + x, sq + St::kOwn + St::kPad + x}, Qout + e0,
                                  qsrc, T0, p, lw, ux, uy, uz);
-  pad_fill<S, kT>(valid, fluid_lanes, __ballot_sync(0xffffffffu, valid), lane, Pout, Qout, e0, p.g);
+  pad_fill<SP, SQ, kT>(valid, fluid_lanes, __ballot_sync(0xffffffffu, valid), lane, Pout, Qout, e0, p.g);
 }
 
-// Arguments of one fused step launch; launch_coupled_step<S> (step_kernels.cuh, one translation unit per storage
-// type) picks the instantiation whose compile-time row length matches the lattice.
+// Arguments of one fused step launch; launch_coupled_step<SP, SQ> (step_kernels.cuh, one translation unit per
+// storage mode) picks the instantiation whose compile-time row length matches the lattice.
 struct StepLaunch {
   const void* Pin;
   void* Pout;
@@ -566,7 +591,7 @@ struct StepLaunch {
   bool macro, own;
   cudaStream_t stream;
 };
-template <typename S>
+template <typename SP, typename SQ>
 void launch_coupled_step(const StepLaunch& a);
 
 // omega and source factors, computed with the device's IEEE division once per lattice

@@ -1,6 +1,6 @@
-// Fused step kernels with float population storage (see step_kernels.cuh).
+// Fused step kernels with float population storage in both lattices (see step_kernels.cuh).
 #include "step_kernels.cuh"
 
 namespace xac {
-template void launch_coupled_step<float>(const StepLaunch&);
+template void launch_coupled_step<float, float>(const StepLaunch&);
 }  // namespace xac

@@ -201,3 +201,30 @@ class Lattice:
         buf = C.create_string_buffer(blob, len(blob))
         with torch.cuda.device(self.device):
             _capi.call("xac_lattice_load_state", self._h, C.addressof(buf), len(blob), stream_ptr(self.device))
+
+
+def reference_run_fp64(mask, steps: int, *, tau_fluid=0.52, heat_power=0.1, t_inlet=25.0, u_inlet_val=0.03,
+                       heat_source=None, Pr=7.0, k_ratio=628.0, rho_outlet=1.0, device="cuda"):
+    """FP64 solve on the GPU (the oracle for the reduced-precision storage forms): cold start, then ``steps``
+    replays of the reference's six-kernel step (src/simulation.py:60-100) in double precision. Returns (rho, u, T)
+    as float64 CUDA tensors in the reference layout."""
+    mask_np = np.ascontiguousarray(np.asarray(mask), dtype=np.int32)
+    if mask_np.ndim != 3:
+        raise ValueError(f"mask must be 3-D (nx, ny, nz), got shape {mask_np.shape}")
+    nx, ny, nz = mask_np.shape
+    hs_np = None
+    if heat_source is not None:
+        hs_np = np.ascontiguousarray(np.array(heat_source, dtype=np.float32))
+        if hs_np.shape != (nx, ny, nz):
+            raise ValueError(f"heat_source shape {hs_np.shape} != domain shape ({nx}, {ny}, {nz})")
+    dev = torch.device(device)
+    d = _capi.Desc(nx, ny, nz, mask_np.ctypes.data, hs_np.ctypes.data if hs_np is not None else None,
+                   float(tau_fluid), float(Pr), float(k_ratio), float(u_inlet_val), float(rho_outlet), float(t_inlet),
+                   float(heat_power), _capi.PRECISIONS["fp32"])
+    rho = torch.empty((nx, ny, nz), dtype=torch.float64, device=dev)
+    u = torch.empty((nx, ny, nz, 3), dtype=torch.float64, device=dev)
+    T = torch.empty((nx, ny, nz), dtype=torch.float64, device=dev)
+    with torch.cuda.device(dev):
+        _capi.call("xac_reference_run_fp64", C.byref(d), int(steps), rho.data_ptr(), u.data_ptr(), T.data_ptr(),
+                   stream_ptr(dev))
+    return rho, u, T

@@ -31,7 +31,8 @@ def run_simulation(mask,
     """src/simulation.py:14-162. Same arguments and the same returned keys
     (u, rho, T as numpy float32 in the reference layout, mask, steps, d_ke, dT_conv, dQ_conv, converged).
 
-    Extra keyword-only arguments: ``precision`` ("fp32", "fp16", "bf16" population storage),
+    Extra keyword-only arguments: ``precision`` (population storage: "fp32"; "fp16" in both
+    lattices; "bf16" fluid with FP16 thermal populations; "fp32_t16" FP32 fluid with FP16 thermal populations),
     ``init_fields`` = (rho, u, T) CUDA tensors to warm-start from, ``keep_lattice`` to also return the
     live :class:`Lattice` under key "lattice" (for device-side scalars), ``min_steps`` > 0 to replace the
     reference's minimum run length before convergence (for warm starts).
