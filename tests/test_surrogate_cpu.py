@@ -1,6 +1,7 @@
 """Host-side logic of the warm-start surrogate on the CPU, with torch's conv3d standing in for the tensor-core
 kernels: network shapes, the training loop, the adjoint-weight identity the data gradient relies on, and the
 mapping between solver fields and the network's channels-last targets."""
+import pytest
 import numpy as np
 import torch
 import torch.nn.functional as F
@@ -117,3 +118,28 @@ def test_convolution_kernels_refuse_host_tensors():
         S.conv_forward(x, w, None, 3)
     with pytest.raises(ValueError, match="CUDA tensor"):
         S.conv_weight_grad(x, x, 3, False)
+
+
+def test_compare_batched_reports_every_design(monkeypatch):
+    """warmstart.compare_batched with the solves replaced by fakes: one row per design that passes the guard, in
+    seed order, with None where either solve did not converge; the guard-tripping designs are skipped when asked."""
+    from xadvcool_b200 import warmstart as W
+
+    def fake_batched(ds, model, *, max_steps, tol, warm_min_steps):
+        n = len(ds)
+        warm = model is not None
+        ok = [not (warm and j == 1) for j in range(n)]  # the second design's warm solve does not converge
+        scal = [{"delta_P": 1.0 + j, "R_th": (2.0 if not warm else 2.02) + j * (tol < 1e-7)} for j in range(n)]
+        steps = [(1000 if warm else 9000) + 100 * j for j in range(n)]
+        return {"wall_s": float(sum(steps)), "designs": n, "converged": sum(ok), "s_per_converged_design": 1.0,
+                "diverged": 0, "steps": steps, "ok": ok, "scalars": scal}
+
+    monkeypatch.setattr(W, "_batched", fake_batched)
+    monkeypatch.setattr(W, "screen", lambda seeds: ([s for s in seeds if s % 3], [s for s in seeds if not s % 3]))
+    monkeypatch.setattr(W, "design", lambda s: (None, None, None, None))
+    r = W.compare_batched(object(), [1, 2, 3, 4, 5], tight_tol=1e-8, solve_cold_tripped=False)
+    rows = r["per_design"]
+    assert [x["seed"] for x in rows] == [1, 2, 4, 5] and r["screened_out"] == 1
+    assert rows[1]["Rth_warm_vs_cold"] is None and rows[1]["Rth_warm_vs_tight"] is None
+    assert rows[0]["Rth_warm_vs_cold"] == pytest.approx(0.01) and rows[0]["cold_steps"] == 9000
+    assert "warm_cold_tripped" not in r and r["compared"] == 3

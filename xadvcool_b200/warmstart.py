@@ -302,12 +302,15 @@ def _vs(a, ref, ok_a, ok_ref):
             "within_half_percent": sum(1 for x, y in zip(dp, rt) if x <= 5e-3 and y <= 5e-3)}
 
 
-def compare_batched(model, seeds, *, max_steps=150000, tol=1e-6, warm_min_steps=1000, tight_tol=None):
+def compare_batched(model, seeds, *, max_steps=150000, tol=1e-6, warm_min_steps=1000, tight_tol=None,
+                    solve_cold_tripped=True):
     """Batched solves of the held-out designs whose cold start passes the divergence guard, cold and warm (same
     designs, same residual): wall seconds per converged design from mask upload to scalars, steps, and the
     scalar agreement per design. The designs whose cold start trips the guard are then solved warm, to count
     those the warm start solves. With ``tight_tol`` the same designs are also solved cold to that residual, and
-    both the cold and the warm scalars are compared with those of the tight solve (``vs_tight``)."""
+    both the cold and the warm scalars are compared with those of the tight solve (``vs_tight``). ``per_design``
+    lists, for every design that passes the guard, its seed, cold and warm steps, and the relative delta_P / R_th
+    differences (warm vs cold; each vs the tight solve when there is one; None where a solve did not converge)."""
     good, bad = screen(seeds)
     out = {"screened_out": len(bad)}
     dg = [design(s) for s in good]
@@ -322,11 +325,24 @@ def compare_batched(model, seeds, *, max_steps=150000, tol=1e-6, warm_min_steps=
                within_half_percent=sum(1 for a, b in zip(dp, rt) if a <= 5e-3 and b <= 5e-3),
                step_ratio=sum(c["steps"]) / max(sum(w["steps"]), 1),
                speedup=c["s_per_converged_design"] / w["s_per_converged_design"])
+    t = None
     if tight_tol is not None:
         t = _batched(dg, None, max_steps=max_steps, tol=tight_tol, warm_min_steps=warm_min_steps)
         out["vs_tight"] = {"tol": tight_tol, "tight_converged": t["converged"],
                            "cold": _vs(c, t, c["ok"], t["ok"]), "warm": _vs(w, t, w["ok"], t["ok"])}
-    if bad:
+
+    def rel(a, b, j, key):
+        return _rel(a["scalars"][j][key], b["scalars"][j][key]) if a["ok"][j] and b["ok"][j] else None
+
+    rows = []
+    for j, s in enumerate(good):
+        r = {"seed": s, "cold_steps": c["steps"][j], "warm_steps": w["steps"][j],
+             "dP_warm_vs_cold": rel(w, c, j, "delta_P"), "Rth_warm_vs_cold": rel(w, c, j, "R_th")}
+        if t is not None:
+            r.update(Rth_cold_vs_tight=rel(c, t, j, "R_th"), Rth_warm_vs_tight=rel(w, t, j, "R_th"))
+        rows.append(r)
+    out["per_design"] = rows
+    if bad and solve_cold_tripped:
         r = _batched([design(s) for s in bad], model, max_steps=max_steps, tol=tol, warm_min_steps=warm_min_steps)
         out["warm_cold_tripped"] = {k: r[k] for k in ("designs", "converged", "diverged", "steps", "wall_s")}
     return out
