@@ -136,7 +136,9 @@ int xac_stats_fields(const float *rho, const float *u, const float *T, const int
  * that loads the library; lattices above 2,097,152 cells are rejected (XAC_EINVAL). The result (XAC_NSTATS
  * doubles) goes to the caller's DEVICE buffer out_dev, asynchronously on `stream`. All calls on a device share
  * the scratch, so calls whose GPU work overlaps race. The first call on a device looks up the scratch address;
- * make it before any stream capture. */
+ * make it before any stream capture. The address is kept for the life of the process: after cudaDeviceReset
+ * (which discards the device's copy of the library's module) this entry point must not be called again in that
+ * process. */
 int xac_stats_fields_noalloc(const float *rho, const float *u, const float *T, const int32_t *mask, int nx, int ny,
                              int nz, double *out_dev, void *stream);
 
