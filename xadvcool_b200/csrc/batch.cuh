@@ -114,14 +114,12 @@ __device__ __forceinline__ void batch_step_tile(const BatchDesign& d, uint32_t t
   const bool valid = x < (uint32_t)d.p.g.nx;
   const uint32_t c = r * (uint32_t)d.p.g.nx + x;
   const uint32_t lw = valid ? __ldg(d.link + c) : ((uint32_t)kSolid << kTypeShift);
-  const unsigned fluid_lanes = __ballot_sync(0xffffffffu, valid && link_type(lw) != kSolid);
   const int lane = threadIdx.x & 31;
-  coupled_cell<SP, SQ, kMacro, kOwn, 1, 0>(c, pop_base(r, x, d.p.g, (int)pitch), (const SP*)d.P[cur],
-                                            (SP*)d.P[cur ^ 1], (const SQ*)d.Q[cur], (SQ*)d.Q[cur ^ 1], d.qsrc, d.u_in,
-                                            d.rho, d.ux, d.uy, d.uz, d.T, d.p, valid, lw,
-                                            (fluid_lanes & sector_group<SP>(lane)) != 0u);
-  pad_fill<SP, SQ, 0>(valid, fluid_lanes, __ballot_sync(0xffffffffu, valid), lane, (SP*)d.P[cur ^ 1],
-                      (SQ*)d.Q[cur ^ 1], pop_base(r, x, d.p.g, (int)pitch), d.p.g);
+  const uint32_t e0 = pop_base(r, x, d.p.g, (int)pitch);
+  coupled_cell<SP, SQ, kMacro, kOwn, 1, 0>(c, r, x, e0, (const SP*)d.P[cur], (SP*)d.P[cur ^ 1], (const SQ*)d.Q[cur],
+                                            (SQ*)d.Q[cur ^ 1], d.qsrc, d.u_in, d.rho, d.ux, d.uy, d.uz, d.T, d.p,
+                                            valid, lw);
+  pad_fill<SQ, 0>(valid, __ballot_sync(0xffffffffu, valid), lane, (SQ*)d.Q[cur ^ 1], e0, d.p.g);
 }
 
 struct BatchRun {

@@ -107,12 +107,20 @@ __global__ void init_state_kernel(const float* __restrict__ rho, const float* __
   const float Tc = T[c];
   const float tx = solid ? 0.0f : vx, ty = solid ? 0.0f : vy, tz = solid ? 0.0f : vz;
   const float usq15t = 1.5f * ((tx * tx + ty * ty) + tz * tz);
+  // fluid populations of non-solid cells only (a solid cell's are w_i: rho = 1 and u = 0 there)
+  uint32_t k = 0;
+  if (!solid) {
+    const uint2 e = p.ftab[ftab_index(p.g, row, x)];
+    k = e.y + (uint32_t)__popc(e.x & ((1u << (x & 31u)) - 1u));
+  }
 #define XAC_INIT(I)                                                                   \
   {                                                                                   \
-    const float fe = feq_term(w_of(I) * r, edotu<I>(vx, vy, vz), usq15);             \
-    const float pc = solid ? fe : fe - omega * (fe - fe);                             \
-    Pop<SP>::st(P0 + e0 + (long long)I * RL, pc, w_of(I));                           \
-    Pop<SP>::st(P1 + e0 + (long long)I * RL, pc, w_of(I));                           \
+    if (!solid) {                                                                     \
+      const float fe = feq_term(w_of(I) * r, edotu<I>(vx, vy, vz), usq15);           \
+      const float pc = fe - omega * (fe - fe);                                        \
+      Pop<SP>::st(P0 + k + (long long)I * p.g.ns, pc, w_of(I));                      \
+      Pop<SP>::st(P1 + k + (long long)I * p.g.ns, pc, w_of(I));                      \
+    }                                                                                 \
     const float ge = feq_term(w_of(I) * Tc, edotu<I>(tx, ty, tz), usq15t);           \
     Pop<SQ>::st(Q0 + e0 + (long long)I * RL, ge, w_of(I) * p.T_ref);                 \
   }
@@ -143,17 +151,17 @@ __global__ void export_fields_kernel(const float* __restrict__ rho, const float*
 __global__ void set_scalar_kernel(float* dst, float v) { *dst = v; }
 
 // Memory-pattern probe of the fused step (SP / SQ: unsigned words of the fluid / thermal storage size): the
-// threads, the link-word reads, the population addresses (fluid pulls with the bounce-back reads its link bits
-// select, thermal pulls from the neighbours) and the whole-sector fills of solid and padding lanes that
-// coupled_step_kernel has, with no arithmetic: every value read is stored unchanged at the cell's own position of
-// the other buffer. Its time is the floor the step's memory access pattern sets. (At the domain faces the thermal
+// threads, the link-word and table reads, the population addresses (fluid pulls of the non-solid cells with the
+// bounce-back reads their link bits select, thermal pulls from the neighbours) and the whole-sector fills of the
+// thermal padding lanes that coupled_step_kernel has, with no arithmetic: every value read is stored unchanged at
+// the cell's own position of the other buffer. Its time is the floor the step's memory access pattern sets. (At the domain faces the thermal
 // rules read the cell's own row instead of a neighbour: the probe pulls there too, which reads padding or guard
 // values.)
 template <typename SP, typename SQ, int kT>
 __global__ void __launch_bounds__(256) pattern_copy_kernel(const SP* __restrict__ Pin, SP* __restrict__ Pout,
                                                            const SQ* __restrict__ Qin, SQ* __restrict__ Qout,
-                                                           const uint32_t* __restrict__ link, Geom g,
-                                                           uint32_t reverse) {
+                                                           const uint32_t* __restrict__ link,
+                                                           const uint2* __restrict__ ftab, Geom g, uint32_t reverse) {
   const int RL = row_len<kT>(g);
   const uint32_t blk = reverse ? gridDim.x - 1u - blockIdx.x : blockIdx.x;
   const uint32_t pos = blk * blockDim.x + threadIdx.x;
@@ -164,17 +172,13 @@ __global__ void __launch_bounds__(256) pattern_copy_kernel(const SP* __restrict_
   const uint32_t c = r * (uint32_t)g.nx + x;
   const uint32_t lw = valid ? __ldg(link + c) : ((uint32_t)kSolid << kTypeShift);
   const bool fluid = valid && link_type(lw) != kSolid;
-  const bool fill_p = (__ballot_sync(0xffffffffu, fluid) & sector_group<SP>(lane)) != 0u;
   const bool fill_q = (__ballot_sync(0xffffffffu, valid) & sector_group<SQ>(lane)) != 0u;
   const uint32_t e0 = pop_base(r, x, g, RL);
   if (fluid) {
-    const Rows<SP, kT> P = rows_at<kT>(Pin, e0, g, RL);
-#define XAC_PC_P(I) Pout[e0 + (I) * RL] = ((lw >> (I)) & 1u) ? __ldg(P.own(opp_of(I))) : __ldg(P.template pull<I>());
+    const FluidAt<SP> P = fluid_at(Pin, r, x, g, ftab);
+#define XAC_PC_P(I) Pout[P.k + (I) * P.ns] = ((lw >> (I)) & 1u) ? __ldg(P.own(opp_of(I))) : __ldg(P.template pull<I>());
     XAC_FOR19(XAC_PC_P)
 #undef XAC_PC_P
-  } else if (fill_p) {
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) Pout[e0 + i * RL] = SP{};
   }
   if (valid) {
     const Rows<SQ, kT> Q = rows_at<kT>(Qin, e0, g, RL);
@@ -192,14 +196,14 @@ template <size_t kBytes>
 using RawWord = typename std::conditional<kBytes == 4, unsigned int, unsigned short>::type;
 
 template <typename SP0, typename SQ0>
-void launch_pattern_copy(const void* Pin, void* Pout, const void* Qin, void* Qout, const uint32_t* link, const Geom& g,
-                         int block, uint32_t reverse, cudaStream_t s) {
+void launch_pattern_copy(const void* Pin, void* Pout, const void* Qin, void* Qout, const uint32_t* link,
+                         const uint2* ftab, const Geom& g, int block, uint32_t reverse, cudaStream_t s) {
   using SP = RawWord<sizeof(SP0)>;
   using SQ = RawWord<sizeof(SQ0)>;
   const unsigned grid = (unsigned)(((long long)g.rows * g.pitch + block - 1) / block);
 #define XAC_PC(KT)                                                                                                 \
   pattern_copy_kernel<SP, SQ, KT><<<grid, block, 0, s>>>((const SP*)Pin, (SP*)Pout, (const SQ*)Qin, (SQ*)Qout, \
-                                                          link, g, reverse)
+                                                          link, ftab, g, reverse)
   switch (g.pitch) {
     case 32: XAC_PC(32); break;
     case 64: XAC_PC(64); break;
@@ -319,6 +323,7 @@ struct LatticeImpl {
   int cur = 0;
   uint8_t* type = nullptr;
   uint32_t* link = nullptr;
+  uint2* ftab = nullptr;  // non-solid cell table of the fluid populations
   float* qsrc = nullptr;
   float* u_in = nullptr;
   float *rho = nullptr, *ux = nullptr, *uy = nullptr, *uz = nullptr, *T = nullptr;
@@ -361,6 +366,7 @@ struct LatticeImpl {
     p.srcf_f = relax[3];
     p.srcf_s = relax[4];
     p.status = status;
+    p.ftab = ftab;
     p.reverse = (uint32_t)cur;  // sweep direction alternates with the buffer parity
     return p;
   }
@@ -373,6 +379,7 @@ struct LatticeImpl {
     for (void* b : {P[0], P[1], Qb[0], Qb[1]}) cudaFree(b);
     cudaFree(type);
     cudaFree(link);
+    cudaFree(ftab);
     cudaFree(qsrc);
     cudaFree(status);
     cudaFree(u_in);
@@ -653,6 +660,32 @@ using namespace xac;
 namespace {
 
 // Normalised heat source times power, internal layout; simulation.py:77-86 and thermal_engine3d.py:116-117.
+// Table of the fluid populations' non-solid cells (FluidAt): per 32-cell word of each row its non-solid mask and
+// the number of non-solid cells before it, with ny + 1 empty rows before and after the grid. Sets g.nt, g.ns and
+// g.np. type is in cell order c = (z*ny + y)*nx + x.
+std::vector<uint2> fluid_table(const uint8_t* type, Geom& g) {
+  g.nt = g.pitch / 32;
+  const long long guard_rows = g.ny + 1;
+  std::vector<uint2> tab((size_t)((g.rows + 2 * guard_rows) * g.nt), make_uint2(0u, 0u));
+  uint32_t k = 0;
+  for (long long r = 0; r < g.rows; ++r)
+    for (int w = 0; w < g.nt; ++w) {
+      uint32_t m = 0;
+      for (int b = 0; b < 32; ++b) {
+        const int x = 32 * w + b;
+        if (x < g.nx && type[r * g.nx + x] != kSolid) m |= 1u << b;
+      }
+      tab[(size_t)((r + guard_rows) * g.nt + w)] = make_uint2(m, k);
+      k += (uint32_t)__builtin_popcount(m);
+    }
+  // rows after the grid: empty words whose count is the total
+  for (size_t t = (size_t)((g.rows + guard_rows) * g.nt); t < tab.size(); ++t) tab[t].y = k;
+  g.ns = ((long long)k + 31) / 32 * 32;
+  if (g.ns == 0) g.ns = 32;
+  g.np = (long long)kQ * g.ns;
+  return tab;
+}
+
 std::vector<float> host_qsrc(const xac_desc* d) {
   const int nx = d->nx, ny = d->ny, nz = d->nz;
   const size_t n = (size_t)nx * ny * nz;
@@ -729,7 +762,8 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
         type[((size_t)z * ny + y) * nx + x] = (uint8_t)m;
       }
   std::vector<float> q = host_qsrc(d);
-  const size_t p_bytes = (size_t)L.g.N * L.p_elem, q_bytes = (size_t)L.g.N * L.q_elem;
+  const std::vector<uint2> ftab = fluid_table(type.data(), L.g);
+  const size_t p_bytes = (size_t)L.g.np * L.p_elem, q_bytes = (size_t)L.g.N * L.q_elem;
   for (int b = 0; b < 2; ++b) {
     XAC_CUDA(cudaMalloc(&L.P[b], p_bytes));
     XAC_CUDA(cudaMalloc(&L.Qb[b], q_bytes));
@@ -737,6 +771,7 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
   int r;
   if ((r = dmalloc(&L.type, n, "alloc type")) != XAC_OK) return r;
   if ((r = dmalloc(&L.link, n, "alloc link")) != XAC_OK) return r;
+  if ((r = dmalloc(&L.ftab, ftab.size(), "alloc fluid table")) != XAC_OK) return r;
   if ((r = dmalloc(&L.qsrc, n, "alloc qsrc")) != XAC_OK) return r;
   if ((r = dmalloc(&L.u_in, 1, "alloc u_in")) != XAC_OK) return r;
   if ((r = dmalloc(&L.status, 1, "alloc status")) != XAC_OK) return r;
@@ -750,12 +785,13 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
   }
   if ((r = dmalloc(&L.red_out, 64, "alloc red_out")) != XAC_OK) return r;
   XAC_CUDA(cudaMallocHost(&L.host_out, 64 * sizeof(double)));
-  // guards and row padding are never used as values; keep them defined
+  // guards, row padding and the unused fluid slots are never used as values; keep them defined
   for (int b = 0; b < 2; ++b) {
     XAC_CUDA(cudaMemsetAsync(L.P[b], 0, p_bytes, s));
     XAC_CUDA(cudaMemsetAsync(L.Qb[b], 0, q_bytes, s));
   }
   XAC_CUDA(cudaMemcpyAsync(L.type, type.data(), n, cudaMemcpyHostToDevice, s));
+  XAC_CUDA(cudaMemcpyAsync(L.ftab, ftab.data(), ftab.size() * sizeof(uint2), cudaMemcpyHostToDevice, s));
   XAC_CUDA(cudaMemcpyAsync(L.qsrc, q.data(), n * sizeof(float), cudaMemcpyHostToDevice, s));
   set_scalar_kernel<<<1, 1, 0, s>>>(L.u_in, L.u_in_host);
   relaxation_factors_kernel<<<1, 1, 0, s>>>((float)L.tau_fluid, L.tau_th_f, L.tau_th_s, (float*)L.red_out);
@@ -927,18 +963,18 @@ int xac_lattice_pattern_copy(xac_lattice* lat, int launches, double* us_per_laun
     const int c = k & 1;
     switch (L.precision) {
       case XAC_FP16:
-        launch_pattern_copy<__half, __half>(L.P[c], L.P[c ^ 1], L.Qb[c], L.Qb[c ^ 1], L.link, L.g, L.tune_block, c, s);
+        launch_pattern_copy<__half, __half>(L.P[c], L.P[c ^ 1], L.Qb[c], L.Qb[c ^ 1], L.link, L.ftab, L.g, L.tune_block, c, s);
         break;
       case XAC_BF16:
-        launch_pattern_copy<__nv_bfloat16, __half>(L.P[c], L.P[c ^ 1], L.Qb[c], L.Qb[c ^ 1], L.link, L.g,
+        launch_pattern_copy<__nv_bfloat16, __half>(L.P[c], L.P[c ^ 1], L.Qb[c], L.Qb[c ^ 1], L.link, L.ftab, L.g,
                                                         L.tune_block, c, s);
         break;
       case XAC_FP32_T16:
-        launch_pattern_copy<float, __half>(L.P[c], L.P[c ^ 1], L.Qb[c], L.Qb[c ^ 1], L.link, L.g, L.tune_block, c,
+        launch_pattern_copy<float, __half>(L.P[c], L.P[c ^ 1], L.Qb[c], L.Qb[c ^ 1], L.link, L.ftab, L.g, L.tune_block, c,
                                                 s);
         break;
       default:
-        launch_pattern_copy<float, float>(L.P[c], L.P[c ^ 1], L.Qb[c], L.Qb[c ^ 1], L.link, L.g, L.tune_block, c, s);
+        launch_pattern_copy<float, float>(L.P[c], L.P[c ^ 1], L.Qb[c], L.Qb[c ^ 1], L.link, L.ftab, L.g, L.tune_block, c, s);
     }
   };
   for (int k = 0; k < 4; ++k) launch(k);  // warm-up
@@ -1032,7 +1068,7 @@ int xac_lattice_validate(xac_lattice* lat, double* out_host, void* stream) {
 int xac_lattice_state_bytes(const xac_lattice* lat, size_t* bytes) {
   XAC_REQUIRE(lat && bytes, "xac_lattice_state_bytes: null pointer");
   const LatticeImpl& L = lat->impl;
-  *bytes = 64 + (size_t)L.g.N * (L.p_elem + L.q_elem) + 5 * (size_t)L.g.ncell * sizeof(float);
+  *bytes = 64 + (size_t)L.g.np * L.p_elem + (size_t)L.g.N * L.q_elem + 5 * (size_t)L.g.ncell * sizeof(float);
   return XAC_OK;
 }
 
@@ -1047,12 +1083,12 @@ int xac_lattice_save_state(xac_lattice* lat, void* host_dst, size_t bytes, void*
   cudaStream_t s = as_stream(stream);
   int r = L.finalize_T(s);
   if (r != XAC_OK) return r;
-  int64_t hdr[8] = {0x58414331, L.g.nx, L.g.ny, L.g.nz, L.precision, L.step, L.own_pending ? 1 : 0, 0};
+  int64_t hdr[8] = {0x58414332, L.g.nx, L.g.ny, L.g.nz, L.precision, L.step, L.own_pending ? 1 : 0, 0};
   float u_in = L.u_in_host;
   std::memcpy(&hdr[7], &u_in, sizeof(float));
   char* dst = (char*)host_dst;
   std::memcpy(dst, hdr, 64);
-  const size_t pb = (size_t)L.g.N * L.p_elem, qb = (size_t)L.g.N * L.q_elem;
+  const size_t pb = (size_t)L.g.np * L.p_elem, qb = (size_t)L.g.N * L.q_elem;
   const size_t nf = (size_t)L.g.ncell * sizeof(float);
   XAC_CUDA(cudaMemcpyAsync(dst + 64, L.P[L.cur], pb, cudaMemcpyDeviceToHost, s));
   XAC_CUDA(cudaMemcpyAsync(dst + 64 + pb, L.Qb[L.cur], qb, cudaMemcpyDeviceToHost, s));
@@ -1071,17 +1107,15 @@ int xac_lattice_load_state(xac_lattice* lat, const void* host_src, size_t bytes,
   LatticeImpl& L = lat->impl;
   int64_t hdr[8];
   std::memcpy(hdr, host_src, 64);
-  XAC_REQUIRE(hdr[0] == 0x58414331 && hdr[1] == L.g.nx && hdr[2] == L.g.ny && hdr[3] == L.g.nz &&
+  XAC_REQUIRE(hdr[0] == 0x58414332 && hdr[1] == L.g.nx && hdr[2] == L.g.ny && hdr[3] == L.g.nz &&
                   hdr[4] == L.precision,
               "xac_lattice_load_state: state was saved from a different lattice");
   std::lock_guard<std::mutex> g(L.mu);
   cudaStream_t s = as_stream(stream);
   const char* src = (const char*)host_src;
-  const size_t pb = (size_t)L.g.N * L.p_elem, qb = (size_t)L.g.N * L.q_elem;
+  const size_t pb = (size_t)L.g.np * L.p_elem, qb = (size_t)L.g.N * L.q_elem;
   const size_t nf = (size_t)L.g.ncell * sizeof(float);
-  // solid cells are read from either buffer, so both get the saved fluid populations
   XAC_CUDA(cudaMemcpyAsync(L.P[0], src + 64, pb, cudaMemcpyHostToDevice, s));
-  XAC_CUDA(cudaMemcpyAsync(L.P[1], src + 64, pb, cudaMemcpyHostToDevice, s));
   XAC_CUDA(cudaMemcpyAsync(L.Qb[0], src + 64 + pb, qb, cudaMemcpyHostToDevice, s));
   float* f[5] = {L.rho, L.ux, L.uy, L.uz, L.T};
   for (int k = 0; k < 5; ++k)
@@ -1844,10 +1878,18 @@ int xac_lattice_footprint(const xac_desc* d, unsigned long long* bytes) {
   const long long n = (long long)d->nx * d->ny * d->nz;
   const long long pitch = (d->nx + 31) / 32 * 32;
   const long long N = ((long long)d->ny * d->nz + 2LL * (d->ny + 2)) * kQ * pitch;
+  // fluid populations of the non-solid cells (all cells when no mask is given)
+  long long nonsolid = n;
+  if (d->mask) {
+    nonsolid = 0;
+    for (long long c = 0; c < n; ++c) nonsolid += d->mask[c] != kSolid;
+  }
+  const long long NP = kQ * ((nonsolid + 31) / 32 * 32 + (nonsolid == 0 ? 32 : 0));
+  const long long ftab = ((long long)d->ny * d->nz + 2LL * (d->ny + 1)) * (pitch / 32) * 8;
   const long long p_elem = (d->precision == XAC_FP32 || d->precision == XAC_FP32_T16) ? 4 : 2;
   const long long q_elem = d->precision == XAC_FP32 ? 4 : 2;
   const long long metric_rows = (long long)reduction_blocks(n) * kNMetrics, stat_rows = stats_tiles(n) * kNStats;
-  *bytes = (unsigned long long)(2 * N * (p_elem + q_elem) + n * (1 + 4 + 4 + 5 * 4) +
+  *bytes = (unsigned long long)(2 * NP * p_elem + 2 * N * q_elem + ftab + n * (1 + 4 + 4 + 5 * 4) +
                                 8 * (metric_rows > stat_rows ? metric_rows : stat_rows) + 64 * 8 + 64);
   return XAC_OK;
 }
