@@ -97,6 +97,35 @@ def test_all_solid_and_all_fluid(cuda):
         assert_exact(ref, rho, u, T)
 
 
+def test_compacted_fluid_slots_at_word_edges_empty_rows_and_solid_west_of_outlet(cuda):
+    """The fluid populations live in slots of the non-solid cells only, found through a per-row table of 32-cell
+    words: rows of three words with solid/fluid flips at the word edges (x = 31/32, 63/64), rows and a whole z slab
+    with no non-solid cell (empty neighbour words), and outlet cells whose x-1 neighbour is solid in every other
+    row (the outlet then copies the solid's rest populations)."""
+    rng = np.random.default_rng(7)
+    nx, ny, nz = 96, 7, 6
+    mask = np.where(rng.random((nx, ny, nz)) < 0.45, 1, 0).astype(np.int32)
+    mask[30:34, :, :] = rng.choice([0, 1], size=(4, ny, nz))
+    mask[62:66, :, :] = rng.choice([0, 1], size=(4, ny, nz))
+    mask[:, 3, :] = 1  # rows with no non-solid cell
+    mask[:, :, 2] = 1  # a slab with none
+    mask[0, :, :] = 2
+    mask[-1, :, :] = 3
+    mask[-2, ::2, :] = 1
+    mask[-2, 1::2, :] = 0
+    kw = dict(tau_fluid=0.62, heat_power=5e-3, u_inlet_val=0.03, Pr=2.5, k_ratio=20.0)
+    hs = np.zeros((nx, ny, nz), np.float32)
+    hs[:, :, 0] = 1.0
+    ref = oracle_fields(mask, 40, hs=hs, **kw)
+    for variant in (0, 1):
+        lat = Lattice(mask, heat_source=hs, **kw)
+        lat.tune(128, variant)
+        lat.step(40)
+        rho, u, T = (a.cpu().numpy() for a in lat.fields())
+        lat.close()
+        assert_exact(ref, rho, u, T)
+
+
 def test_stats_match_oracle(cuda):
     mask, hs = channel(12)
     kw = dict(tau_fluid=0.6, heat_power=1e-3, u_inlet_val=0.05, Pr=2.0, k_ratio=20.0)

@@ -268,21 +268,21 @@ __device__ __forceinline__ FluidAt<S> fluid_at(const S* base, uint32_t r, uint32
 
 #define XAC_FOR19(M) M(0) M(1) M(2) M(3) M(4) M(5) M(6) M(7) M(8) M(9) M(10) M(11) M(12) M(13) M(14) M(15) M(16) M(17) M(18)
 
-// Lanes sharing one 32-byte DRAM sector of a population row (rows start on 32-value boundaries).
+// Lanes sharing one 32-byte DRAM sector of a thermal population row (rows start on 32-value boundaries).
 template <typename S>
 __device__ __forceinline__ unsigned sector_group(int lane) {
   return sizeof(S) == 4 ? (0xFFu << (lane & ~7)) : (0xFFFFu << (lane & ~15));
 }
 
 // The three parts of one coupled step of cell c (see the scheme at the top of this file). Solid cells carry no
-// fluid work: their fluid populations are the rest equilibrium w_i for ever (fluid_engine3d.py:193-194 never
-// streams them, and they start at rho=1, u=0); a solid lane still stores w_i when a fluid lane shares its
-// sector, so every sector of the fluid output is written whole.
-// c is the compact cell index (link word, heat source, fields); P/Q are the cell's row pointers into the input
-// populations and Po/Qo its own position in the outputs. Direction i of the cell is at +i*pitch.
+// fluid work and store no fluid populations: theirs are the rest equilibrium w_i for ever
+// (fluid_engine3d.py:193-194 never streams them, and they start at rho=1, u=0).
+// c is the cell index (link word, heat source, fields); P is the cell's view of the input fluid populations and
+// Po its own slot in the output (direction i at +i*ns); Q is its row view of the input thermal populations and Qo
+// its own position in the output (direction i at +i*pitch).
 
 // fluid lattice of a non-solid cell: pull with the boundary rules, moments, BGK collision; returns u
-template <typename S, bool kMacro, int kLd, int kT, class Acc>
+template <typename S, bool kMacro, int kLd, class Acc>
 __device__ __forceinline__ void fluid_cell(const uint32_t c, const Acc& P, S* __restrict__ Po,
                                            const float* __restrict__ u_in_ptr, float* __restrict__ rho_o,
                                            float* __restrict__ ux_o, float* __restrict__ uy_o,
@@ -496,7 +496,7 @@ __device__ __forceinline__ void coupled_cell(const uint32_t c, const uint32_t r,
   float ux = 0.0f, uy = 0.0f, uz = 0.0f;
   if (fluid) {
     const FluidAt<SP> P = fluid_at(Pin, r, x, p.g, p.ftab);
-    fluid_cell<SP, kMacro, kLd, kT>(c, P, Pout + P.k, u_in_ptr, rho_o, ux_o, uy_o, uz_o, p, lw, ux, uy, uz);
+    fluid_cell<SP, kMacro, kLd>(c, P, Pout + P.k, u_in_ptr, rho_o, ux_o, uy_o, uz_o, p, lw, ux, uy, uz);
   } else if (valid) {
     solid_cell<kMacro>(c, rho_o, ux_o, uy_o, uz_o);
   }
@@ -519,7 +519,7 @@ __device__ __forceinline__ void pad_fill(bool valid, unsigned valid_lanes, int l
 
 // One thread per row position: block-consecutive threads walk x along a row (a warp never spans two rows, the
 // row length being a multiple of 32); positions x >= nx are padding. kT > 0 makes the row length and every
-// population offset compile-time constants; kT = 0 reads it from the geometry.
+// thermal population offset compile-time constants; kT = 0 reads it from the geometry.
 template <typename SP, typename SQ, bool kMacro, bool kOwn, int kT>
 __global__ void __launch_bounds__(256) coupled_step_kernel(const SP* __restrict__ Pin, SP* __restrict__ Pout,
                                                            const SQ* __restrict__ Qin, SQ* __restrict__ Qout,
@@ -628,7 +628,7 @@ __global__ void __launch_bounds__(kT) coupled_qstage_kernel(const SP* __restrict
   float ux = 0.0f, uy = 0.0f, uz = 0.0f;
   if (valid && link_type(lw) != kSolid) {
     const FluidAt<SP> P = fluid_at(Pin, r, x, p.g, p.ftab);
-    fluid_cell<SP, kMacro, 0, kT>(c, P, Pout + P.k, u_in_ptr, rho_o, ux_o, uy_o, uz_o, p, lw, ux, uy, uz);
+    fluid_cell<SP, kMacro, 0>(c, P, Pout + P.k, u_in_ptr, rho_o, ux_o, uy_o, uz_o, p, lw, ux, uy, uz);
   } else if (valid) {
     solid_cell<kMacro>(c, rho_o, ux_o, uy_o, uz_o);
   }

@@ -1,6 +1,6 @@
-// Dispatch of the fused step over compile-time row lengths (each instantiation makes every population offset
-// an immediate). Included once per storage mode (fluid storage SP, thermal storage SQ) by step_f32.cu /
-// step_f16.cu / step_bf16.cu, which compile in parallel.
+// Dispatch of the fused step over compile-time row lengths (each instantiation makes every thermal population
+// offset an immediate). Included once per storage mode (fluid storage SP, thermal storage SQ) by step_f32.cu /
+// step_f16.cu / step_bf16.cu / step_f32t16.cu, which compile in parallel.
 #pragma once
 
 #include "lattice_kernels.cuh"
