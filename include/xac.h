@@ -290,6 +290,10 @@ int xac_scalars_fields(const float *rho, const float *u, const float *T, const i
 #define XAC_NVALIDATE 16
 int xac_lattice_validate(xac_lattice *lat, double *out_host, void *stream);
 
+/* The lattice's own restart format: a 64-byte header (tag "XAC2", size, precision, step count, inlet velocity,
+ * number of non-solid cells), the fluid populations of the non-solid cells, the thermal populations and the
+ * fields rho, u, T. A state loads only into a lattice of the same size, precision and non-solid cell count, that is
+ * one made from the same mask. */
 int xac_lattice_state_bytes(const xac_lattice *lat, size_t *bytes);
 int xac_lattice_save_state(xac_lattice *lat, void *host_dst, size_t bytes, void *stream);
 int xac_lattice_load_state(xac_lattice *lat, const void *host_src, size_t bytes, void *stream);

@@ -182,6 +182,21 @@ def test_save_load_roundtrip(cuda):
         assert np.array_equal(x, y)
 
 
+def test_state_from_another_mask_is_refused(cuda):
+    """Fluid populations are stored per non-solid cell, so a state only means something for the mask it was saved
+    from: a lattice of the same size with another mask refuses it."""
+    mask, hs = channel(16)
+    other, _ = channel(17)
+    assert (other == 1).sum() != (mask == 1).sum()
+    kw = dict(tau_fluid=0.6, heat_power=1e-3, u_inlet_val=0.04, Pr=2.0, k_ratio=20.0, heat_source=hs)
+    lat = Lattice(mask, **kw)
+    lat.step(5)
+    blob = lat.save_state()
+    lat2 = Lattice(other, **kw)
+    with pytest.raises(Exception, match="different lattice"):
+        lat2.load_state(blob)
+
+
 def test_warm_start_matches_oracle(cuda):
     mask, hs = channel(17)
     kw = dict(tau_fluid=0.6, heat_power=1e-3, u_inlet_val=0.04, Pr=2.0, k_ratio=20.0)

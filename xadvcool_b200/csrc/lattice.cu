@@ -324,6 +324,7 @@ struct LatticeImpl {
   uint8_t* type = nullptr;
   uint32_t* link = nullptr;
   uint2* ftab = nullptr;  // non-solid cell table of the fluid populations
+  uint32_t nonsolid = 0;  // non-solid cells (the fluid populations' slots in use)
   float* qsrc = nullptr;
   float* u_in = nullptr;
   float *rho = nullptr, *ux = nullptr, *uy = nullptr, *uz = nullptr, *T = nullptr;
@@ -663,7 +664,7 @@ namespace {
 // Table of the fluid populations' non-solid cells (FluidAt): per 32-cell word of each row its non-solid mask and
 // the number of non-solid cells before it, with ny + 1 empty rows before and after the grid. Sets g.nt, g.ns and
 // g.np. type is in cell order c = (z*ny + y)*nx + x.
-std::vector<uint2> fluid_table(const uint8_t* type, Geom& g) {
+std::vector<uint2> fluid_table(const uint8_t* type, Geom& g, uint32_t* nonsolid) {
   g.nt = g.pitch / 32;
   const long long guard_rows = g.ny + 1;
   std::vector<uint2> tab((size_t)((g.rows + 2 * guard_rows) * g.nt), make_uint2(0u, 0u));
@@ -680,6 +681,7 @@ std::vector<uint2> fluid_table(const uint8_t* type, Geom& g) {
     }
   // rows after the grid: empty words whose count is the total
   for (size_t t = (size_t)((g.rows + guard_rows) * g.nt); t < tab.size(); ++t) tab[t].y = k;
+  *nonsolid = k;
   g.ns = ((long long)k + 31) / 32 * 32;
   if (g.ns == 0) g.ns = 32;
   g.np = (long long)kQ * g.ns;
@@ -762,7 +764,7 @@ int create_impl(const xac_desc* d, LatticeImpl& L, cudaStream_t s) {
         type[((size_t)z * ny + y) * nx + x] = (uint8_t)m;
       }
   std::vector<float> q = host_qsrc(d);
-  const std::vector<uint2> ftab = fluid_table(type.data(), L.g);
+  const std::vector<uint2> ftab = fluid_table(type.data(), L.g, &L.nonsolid);
   const size_t p_bytes = (size_t)L.g.np * L.p_elem, q_bytes = (size_t)L.g.N * L.q_elem;
   for (int b = 0; b < 2; ++b) {
     XAC_CUDA(cudaMalloc(&L.P[b], p_bytes));
@@ -1086,6 +1088,7 @@ int xac_lattice_save_state(xac_lattice* lat, void* host_dst, size_t bytes, void*
   int64_t hdr[8] = {0x58414332, L.g.nx, L.g.ny, L.g.nz, L.precision, L.step, L.own_pending ? 1 : 0, 0};
   float u_in = L.u_in_host;
   std::memcpy(&hdr[7], &u_in, sizeof(float));
+  std::memcpy(reinterpret_cast<char*>(&hdr[7]) + 4, &L.nonsolid, sizeof(uint32_t));
   char* dst = (char*)host_dst;
   std::memcpy(dst, hdr, 64);
   const size_t pb = (size_t)L.g.np * L.p_elem, qb = (size_t)L.g.N * L.q_elem;
@@ -1107,9 +1110,11 @@ int xac_lattice_load_state(xac_lattice* lat, const void* host_src, size_t bytes,
   LatticeImpl& L = lat->impl;
   int64_t hdr[8];
   std::memcpy(hdr, host_src, 64);
+  uint32_t nonsolid = 0;
+  std::memcpy(&nonsolid, reinterpret_cast<const char*>(&hdr[7]) + 4, sizeof(uint32_t));
   XAC_REQUIRE(hdr[0] == 0x58414332 && hdr[1] == L.g.nx && hdr[2] == L.g.ny && hdr[3] == L.g.nz &&
-                  hdr[4] == L.precision,
-              "xac_lattice_load_state: state was saved from a different lattice");
+                  hdr[4] == L.precision && nonsolid == L.nonsolid,
+              "xac_lattice_load_state: state was saved from a different lattice (size, precision or mask)");
   std::lock_guard<std::mutex> g(L.mu);
   cudaStream_t s = as_stream(stream);
   const char* src = (const char*)host_src;
