@@ -408,7 +408,8 @@ int xac_batch_launch_counts(const xac_batch *batch, long long *graph_launches, l
  * took part in, shared among the designs of each launch in proportion to their cells. slots / results /
  * gpu_seconds must hold xac_batch_size() entries. A finished design keeps its lattice (xac_batch_lattice: fields,
  * stats, scalars) until xac_batch_release frees its slot and device memory. xac_lattice_footprint gives the
- * device bytes a design will take, for admission under a memory budget. */
+ * device bytes a design will take, for admission under a memory budget; it reads design->mask when given, since
+ * fluid populations are stored for the non-solid cells only (without a mask every cell counts). */
 int xac_batch_open(int precision, xac_batch **out);
 int xac_batch_admit(xac_batch *batch, const xac_desc *design, int *slot, void *stream);
 int xac_batch_advance(xac_batch *batch, const xac_run_opts *opts, long long steps, int *n_finished, int *slots,

@@ -21,6 +21,22 @@ def test_shard_is_a_balanced_partition():
     assert sweep.shard(costs, 2) == sweep.shard(costs, 2)  # deterministic
 
 
+def test_footprint_counts_fluid_populations_of_non_solid_cells_only():
+    """The queue's memory budget uses the library's footprint: fluid populations (two buffers, 19 per cell) are
+    stored for the mask's non-solid cells, in slots rounded up to 32, so a solid cell costs 2 x 19 population
+    bytes less than a fluid one. No GPU is needed: the figure is host arithmetic."""
+    from xadvcool_b200.batch import footprint
+    shape = (10, 6, 5)  # 300 cells: 320 slots all fluid, 32 (the minimum) all solid
+    fluid = dict(mask=np.zeros(shape, np.int32))
+    solid = dict(mask=np.ones(shape, np.int32))
+    for precision, pop_bytes in (("fp32", 4), ("fp16", 2), ("bf16", 2), ("fp32_t16", 4)):
+        diff = footprint(fluid, precision) - footprint(solid, precision)
+        assert diff == 2 * 19 * pop_bytes * (320 - 32), precision
+    half = np.zeros(shape, np.int32)
+    half[:, :3, :] = 1  # 150 solid cells: 150 non-solid, 160 slots
+    assert footprint(fluid) - footprint(dict(mask=half)) == 2 * 19 * 4 * (320 - 160)
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))

@@ -50,11 +50,16 @@ def _desc(d: dict, i, precision: str):
 
 
 def footprint(design: dict, precision: str = "fp32") -> int:
-    """Device bytes a design takes in a batch (populations, link words, fields, reduction rows)."""
+    """Device bytes a design takes in a batch (populations, link words, fields, reduction rows). Fluid populations
+    are stored for the mask's non-solid cells only, so the mask is read."""
     if precision not in _capi.PRECISIONS:
         raise ValueError(f"precision must be one of {sorted(_capi.PRECISIONS)}")
-    nx, ny, nz = np.asarray(design["mask"]).shape
-    d = _capi.Desc(nx, ny, nz, None, None, 0.6, 1.0, 1.0, 0.0, 1.0, 0.0, 0.0, _capi.PRECISIONS[precision])
+    mask = np.ascontiguousarray(np.asarray(design["mask"]), dtype=np.int32)
+    if mask.ndim != 3:
+        raise ValueError("mask must be 3-D")
+    nx, ny, nz = mask.shape
+    d = _capi.Desc(nx, ny, nz, mask.ctypes.data, None, 0.6, 1.0, 1.0, 0.0, 1.0, 0.0, 0.0,
+                   _capi.PRECISIONS[precision])
     out = C.c_ulonglong()
     _capi.call("xac_lattice_footprint", C.byref(d), C.byref(out))
     return int(out.value)
