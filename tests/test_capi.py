@@ -75,3 +75,19 @@ def test_invalid_arguments_are_reported_without_touching_the_gpu():
         _capi.check(rc)
     rc = lib.xac_equilibrium(None, None, None, 0, 1, 1, None)
     assert rc == _capi.XAC_EINVAL and b"positive" in lib.xac_last_error()
+
+
+def test_autotune_cache_is_keyed_on_the_library_build(tmp_path, monkeypatch):
+    """Launch shapes timed on one build of libxac.so are not reused by another: the cache key holds a hash of the
+    library file, so a rebuilt kernel or a new population layout is timed afresh."""
+    import shutil
+    from xadvcool_b200 import autotune
+    first = autotune._lib_id()
+    assert re.fullmatch(r"[0-9a-f]{12}", first) and autotune._lib_id() == first
+    copy = tmp_path / "libxac.so"
+    shutil.copyfile(_capi.LIB_PATH, copy)
+    with open(copy, "ab") as f:
+        f.write(b"\0")  # another build
+    monkeypatch.setattr(_capi, "LIB_PATH", copy)
+    monkeypatch.setattr(autotune, "_LIB_ID", None)
+    assert autotune._lib_id() != first

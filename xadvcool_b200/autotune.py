@@ -3,8 +3,9 @@ tile of the persistent batched kernel.
 
 The shape changes only the schedule, never a result (every cell runs the same arithmetic). Candidates are
 timed with CUDA events on a scratch lattice built from the same inputs, so the caller's lattice does not
-advance. The winner is cached per (device, lattice shape, precision, solid fraction) in a JSON file
-(``$XAC_AUTOTUNE_CACHE``, default ``~/.cache/xadvcool_b200/autotune.json``).
+advance. The winner is cached per (device, library build, lattice shape, precision, solid fraction) in a JSON
+file (``$XAC_AUTOTUNE_CACHE``, default ``~/.cache/xadvcool_b200/autotune.json``). The library build is a hash of
+libxac.so, so shapes timed on other kernels (an older build, another layout) are never reused.
 """
 from __future__ import annotations
 
@@ -23,9 +24,26 @@ def _cache_path() -> Path:
     return Path(os.environ.get("XAC_AUTOTUNE_CACHE", Path.home() / ".cache" / "xadvcool_b200" / "autotune.json"))
 
 
+_LIB_ID = None
+
+
+def _lib_id() -> str:
+    """Short hash of the loaded library file (computed once per process)."""
+    global _LIB_ID
+    if _LIB_ID is None:
+        import hashlib
+        from . import _capi
+        h = hashlib.sha256()
+        with open(_capi.LIB_PATH, "rb") as f:
+            for chunk in iter(lambda: f.read(1 << 20), b""):
+                h.update(chunk)
+        _LIB_ID = h.hexdigest()[:12]
+    return _LIB_ID
+
+
 def _key(device, shape, precision, solid_frac) -> str:
     name = torch.cuda.get_device_name(device).replace(" ", "_")
-    return f"{name}|{shape[0]}x{shape[1]}x{shape[2]}|{precision}|solid{round(solid_frac, 1):.1f}"
+    return f"{name}|lib{_lib_id()}|{shape[0]}x{shape[1]}x{shape[2]}|{precision}|solid{round(solid_frac, 1):.1f}"
 
 
 def _load_cache() -> dict:
@@ -122,7 +140,7 @@ def autotune_batch(designs, *, precision="fp32", device="cuda", steps=300, use_c
     cells = sum(int(np.asarray(d["mask"]).size) for d in designs)
     solid = sum(int((np.asarray(d["mask"]) == 1).sum()) for d in designs) / max(cells, 1)
     name = torch.cuda.get_device_name(dev).replace(" ", "_")
-    key = f"batch|{name}|{len(designs)}|{cells}|{precision}|solid{round(solid, 2):.2f}"
+    key = f"batch|{name}|lib{_lib_id()}|{len(designs)}|{cells}|{precision}|solid{round(solid, 2):.2f}"
     cache = _load_cache() if use_cache else {}
     if key in cache:
         return cache[key]
