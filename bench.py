@@ -548,9 +548,10 @@ def run_gpu_arm(args):
                              "alg_bytes_per_launch": alg_bytes, "mean_launch_us": round(step_ms * 1e3, 3),
                              "pattern_floor": {"us_per_launch": round(pattern_us, 3),
                                                "step_frac": round(pattern_us / (step_ms * 1e3), 4),
-                                               "what": "the step's loads and stores (same addresses, solid "
-                                                       "skips, sector fills) with no arithmetic, timed on the "
-                                                       "same lattice: step_frac = floor / step time"}},
+                                               "what": "the step's loads and stores (same addresses: fluid "
+                                                       "slots of the non-solid cells, thermal rows and padding "
+                                                       "fills) with no arithmetic, timed on the same lattice: "
+                                                       "step_frac = floor / step time"}},
                 "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "s_per_solve": round(e2e_max, 4),
                         "solves_s": [round(x, 4) for x in solve_s],

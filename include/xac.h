@@ -240,8 +240,8 @@ int xac_lattice_tune(xac_lattice *lat, int block, int variant);
 int xac_lattice_get_tune(const xac_lattice *lat, int *block, int *variant);
 /* Diagnostic, no reference counterpart: the floor that the fused step's memory access pattern sets for this
  * lattice. Times `launches` launches of a kernel with the step's threads (the lattice's block size, one thread per
- * row position, the alternating sweep), link-word reads, population addresses (fluid pulls with the bounce-back
- * reads, thermal pulls, solid cells' fluid populations skipped, whole-sector fills) and no arithmetic: each value
+ * row position, the alternating sweep), link-word and slot-table reads, population addresses (fluid pulls of the
+ * non-solid cells with the bounce-back reads, thermal pulls, thermal padding fills) and no arithmetic: each value
  * read is stored unchanged. CUDA events on `stream`, after 4 untimed launches. The copies are not a physical state,
  * so the lattice is re-initialised to the cold start (step 0) afterwards. */
 int xac_lattice_pattern_copy(xac_lattice *lat, int launches, double *us_per_launch, void *stream);
